@@ -1,0 +1,976 @@
+// Host runtime and C ABI of the B200 transform engine (include/b200fft.h).
+//
+// A handle is one ParaFaFT backend object (backend/fft_backend.hpp:45-196):
+// it owns a stream, the per-stage C2C plans, the in-place R2C/C2R plans and
+// the twiddle tables, and it holds back two kinds of work so that it can fuse
+// them:
+//   * a device-to-device memcpy (ParaFaFT's single-rank exchange_local,
+//     parafaft_common.hpp:467-543) whose destination the next transform reads
+//     is folded into that transform: the kernel reads the copy's source and
+//     writes the destination;
+//   * execute_stage calls of a middle-axis stage on consecutive slices (the
+//     leading-dimension loop, parafaft_c2c.hpp:875-896,
+//     parafaft_r2c.hpp:1224-1244) accumulate into one launch that starts when
+//     the loop's last slice arrives.
+// The number of slices of such a loop is inferred from the plans: a stage plan
+// of ParaFaFT's middle-axis form (stride == batch, dist == 1) whose
+// length*batch divides the element count of the full stage buffer (the largest
+// length*batch over all plans; (N/2+1)*batch for R2C) covers total/(length*batch)
+// slices.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/b200fft.h"
+#include "fft_common.hpp"
+#include "launch.hpp"
+
+using namespace b200fft;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(B200FFT_ERR_CUDA, std::string("CUDA error in ") + what + ": " +
+                                    cudaGetErrorString(e));
+}
+
+#define B2_TRY(expr)                                                           \
+  do {                                                                         \
+    int rc_ = (expr);                                                          \
+    if (rc_ != B200FFT_SUCCESS)                                                \
+      return rc_;                                                              \
+  } while (0)
+
+bool env_flag(const char *name) {
+  const char *v = std::getenv(name);
+  return v != nullptr && v[0] != '\0' && v[0] != '0';
+}
+
+// Kernel choice of a plan.
+struct Choice {
+  int family = 0; // 0 static, 1 generic
+  bool col = false;
+  int L = 0;      // complex points of the stage loop
+  int tlen = 0;   // twiddle table length
+  int TB = 0, NT = 0;
+  GenArgs gen{};
+};
+
+struct Plan {
+  bool valid = false;
+  int kind = KIND_C2C;
+  int len = 0;
+  long long batch = 0, stride = 0, dist = 0;
+  Choice ch;
+};
+
+struct HeldCopy {
+  bool active = false;
+  char *dst = nullptr;
+  const char *src = nullptr;
+  size_t bytes = 0;
+};
+
+struct HeldRun {
+  bool active = false;
+  int stage = -1;
+  int dir = 0;
+  char *out0 = nullptr;
+  long long count = 0;
+  long long lead = 1;
+  size_t slab_bytes = 0;
+  bool fused = false;
+};
+
+// Factor a length for the generic kernel: 8s, one 4 or 2, 5s, 3s, then other
+// primes up to kGenMaxPrime. Returns false for an unsupported length.
+bool gen_schedule(int L, int *rad, int *nst) {
+  int m = L, k = 0;
+  auto push = [&](int r) -> bool {
+    if (k >= kGenMaxStages)
+      return false;
+    rad[k++] = r;
+    m /= r;
+    return true;
+  };
+  while (m % 8 == 0)
+    if (!push(8)) return false;
+  if (m % 4 == 0 && !push(4)) return false;
+  if (m % 2 == 0 && !push(2)) return false;
+  while (m % 5 == 0)
+    if (!push(5)) return false;
+  while (m % 3 == 0)
+    if (!push(3)) return false;
+  for (int p = 7; p <= kGenMaxPrime && m > 1; p += 2) {
+    while (m % p == 0)
+      if (!push(p)) return false;
+  }
+  *nst = k;
+  return m == 1;
+}
+
+int ilog2(int x) {
+  int l = 0;
+  while ((1 << l) < x)
+    ++l;
+  return l;
+}
+
+// Choose the kernel for a plan. kind: KIND_C2C/R2C/C2R.
+int choose_kernel(int prec, int kind, int len, long long batch, long long stride,
+                  long long dist, bool force_generic, Choice *out) {
+  const int csize = prec == B200FFT_F64 ? 16 : 8;
+  Choice ch;
+  int L = len;
+  bool odd = false;
+  if (kind == KIND_C2C) {
+    ch.col = dist < stride;
+    ch.tlen = len;
+  } else {
+    odd = (len % 2) != 0;
+    L = odd ? len : len / 2;
+    ch.col = false;
+    ch.tlen = len;
+  }
+  ch.L = L;
+  const bool static_ok =
+      !force_generic && static_length_ok(L) &&
+      (kind == KIND_C2C || (!odd && stride == 1 && dist % 2 == 0 && L <= 2048));
+  if (static_ok) {
+    const CfgS c = cfg_static(csize, L, ch.col);
+    ch.family = 0;
+    ch.TB = c.TB;
+    ch.NT = c.NT;
+    *out = ch;
+    return B200FFT_SUCCESS;
+  }
+  // generic
+  GenArgs &g = ch.gen;
+  std::memset(&g, 0, sizeof(g));
+  if (!gen_schedule(L, g.rad, &g.nst))
+    return fail(B200FFT_ERR_UNSUPPORTED,
+                "b200fft: length " + std::to_string(len) +
+                    " has a prime factor above " + std::to_string(kGenMaxPrime) +
+                    "; no kernel for it");
+  const size_t one = 2ull * L * csize;
+  if (one > kGenericSmemLimit)
+    return fail(B200FFT_ERR_UNSUPPORTED,
+                "b200fft: length " + std::to_string(len) +
+                    " exceeds the single-pass limit of the generic kernel");
+  int TB = 1;
+  const size_t target = 48 * 1024;
+  while (TB < 64 && one * (2 * TB) <= target)
+    TB *= 2;
+  g.L = L;
+  g.nreal = kind == KIND_C2C ? 0 : len;
+  g.odd = odd ? 1 : 0;
+  if (kind == KIND_C2C)
+    g.lout = L;
+  else if (kind == KIND_R2C)
+    g.lout = odd ? len / 2 + 1 : L + 1;
+  else
+    g.lout = odd ? len : L;
+  g.TB = TB;
+  g.logTB = ilog2(TB);
+  g.tscale = (kind != KIND_C2C && !odd) ? 2 : 1;
+  int p = 1;
+  for (int s = 0; s < g.nst; ++s) {
+    g.nsv[s] = p;
+    g.ns[s] = make_fastdiv(static_cast<uint32_t>(p));
+    g.bq[s] = make_fastdiv(static_cast<uint32_t>(L / g.rad[s]));
+    p *= g.rad[s];
+  }
+  g.Ldiv = make_fastdiv(static_cast<uint32_t>(L));
+  g.Loutdiv = make_fastdiv(static_cast<uint32_t>(g.lout));
+  ch.family = 1;
+  ch.TB = TB;
+  ch.NT = kGenThreads;
+  *out = ch;
+  return B200FFT_SUCCESS;
+}
+
+std::string describe_choice(const Choice &ch, int kind) {
+  char buf[256];
+  std::string rad;
+  if (ch.family == 0) {
+    int m = ch.L;
+    std::vector<int> r;
+    while (m % 8 == 0 && m > 1) { r.push_back(8); m /= 8; }
+    if (m % 4 == 0) { r.push_back(4); m /= 4; }
+    if (m % 2 == 0) { r.push_back(2); m /= 2; }
+    for (size_t i = 0; i < r.size(); ++i)
+      rad += (i ? "x" : "") + std::to_string(r[i]);
+  } else {
+    for (int s = 0; s < ch.gen.nst; ++s)
+      rad += (s ? "x" : "") + std::to_string(ch.gen.rad[s]);
+  }
+  if (rad.empty())
+    rad = "1";
+  const char *kn = kind == KIND_C2C ? "c2c" : (kind == KIND_R2C ? "r2c" : "c2r");
+  std::snprintf(buf, sizeof(buf), "%s %s L=%d %s tb=%d nt=%d radices=%s",
+                ch.family == 0 ? "static" : "generic", kn, ch.L,
+                ch.col ? "col" : "row", ch.TB, ch.NT, rad.c_str());
+  return buf;
+}
+
+std::mutex g_alloc_mu;
+
+} // namespace
+
+struct b200fft_handle_s {
+  int prec = B200FFT_F32;
+  int rsize = 4; // bytes of FloatType
+  int nstages = 0;
+  int plan_flag = 0;
+  unsigned flags = 0;
+  bool record_only = false;
+  bool defer = true;
+  bool force_generic = false;
+  int device = -1;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  std::vector<Plan> stages;
+  Plan r2c, c2r;
+  std::map<int, void *> tables;
+  HeldCopy copy;
+  HeldRun run;
+  b200fft_stats stats{};
+  std::deque<b200fft_launch_record> log;
+  // per-launch timing
+  bool profiling = false;
+  struct Timed {
+    size_t seq;
+    cudaEvent_t a, b;
+  };
+  std::deque<Timed> timed;
+  std::vector<cudaEvent_t> event_pool;
+  size_t seq = 0;        // sequence number of the next log record
+  size_t log_base = 0;   // sequence number of log.front()
+
+  size_t csize() const { return 2 * static_cast<size_t>(rsize); }
+};
+
+namespace {
+
+using H = b200fft_handle_s;
+
+void push_log(H *h, b200fft_launch_record r) {
+  r.ms = -1.0;
+  h->log.push_back(r);
+  h->seq++;
+  if (h->log.size() > 4096) {
+    h->log.pop_front();
+    h->log_base++;
+  }
+}
+
+cudaEvent_t take_event(H *h) {
+  if (!h->event_pool.empty()) {
+    cudaEvent_t e = h->event_pool.back();
+    h->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return e;
+}
+
+// Bracket the next device operation with events when profiling.
+struct ProfileScope {
+  H *h;
+  cudaEvent_t a = nullptr;
+  explicit ProfileScope(H *hh) : h(hh) {
+    if (h->profiling && !h->record_only) {
+      a = take_event(h);
+      if (a)
+        cudaEventRecord(a, h->stream);
+    }
+  }
+  // call after push_log of the operation's record
+  void done() {
+    if (!a)
+      return;
+    cudaEvent_t b = take_event(h);
+    if (!b) {
+      h->event_pool.push_back(a);
+      return;
+    }
+    cudaEventRecord(b, h->stream);
+    h->timed.push_back({h->seq - 1, a, b});
+    a = nullptr;
+  }
+};
+
+// Resolve pending timings into the log (blocks on the events).
+void resolve_timings(H *h) {
+  while (!h->timed.empty()) {
+    auto t = h->timed.front();
+    h->timed.pop_front();
+    float ms = -1.0f;
+    if (cudaEventSynchronize(t.b) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
+      if (t.seq >= h->log_base && t.seq - h->log_base < h->log.size())
+        h->log[t.seq - h->log_base].ms = ms;
+    } else {
+      cudaGetLastError();
+    }
+    h->event_pool.push_back(t.a);
+    h->event_pool.push_back(t.b);
+  }
+}
+
+int get_table(H *h, int n, const void **out) {
+  if (h->record_only) {
+    *out = nullptr;
+    return B200FFT_SUCCESS;
+  }
+  auto it = h->tables.find(n);
+  if (it != h->tables.end()) {
+    *out = it->second;
+    return B200FFT_SUCCESS;
+  }
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, static_cast<size_t>(n) * h->csize());
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaMalloc (twiddle table)");
+  if (h->prec == B200FFT_F64)
+    e = launch_twiddle_table(static_cast<double2 *>(p), nullptr, n, h->stream);
+  else
+    e = launch_twiddle_table(nullptr, static_cast<float2 *>(p), n, h->stream);
+  if (e != cudaSuccess) {
+    cudaFree(p);
+    return cuda_fail(e, "twiddle table kernel");
+  }
+  h->tables[n] = p;
+  *out = p;
+  return B200FFT_SUCCESS;
+}
+
+// Elements (complex) in the largest stage buffer any plan covers.
+long long full_elems(const H *h) {
+  long long t = 0;
+  for (const Plan &p : h->stages)
+    if (p.valid)
+      t = std::max(t, static_cast<long long>(p.len) * p.batch);
+  if (h->r2c.valid)
+    t = std::max(t, static_cast<long long>(h->r2c.len / 2 + 1) * h->r2c.batch);
+  if (h->c2r.valid)
+    t = std::max(t, static_cast<long long>(h->c2r.len / 2 + 1) * h->c2r.batch);
+  return t;
+}
+
+long long infer_lead(const H *h, const Plan &p) {
+  if (!h->defer)
+    return 1;
+  if (p.dist != 1 || p.stride != p.batch)
+    return 1;
+  const long long slab = static_cast<long long>(p.len) * p.batch;
+  const long long t = full_elems(h);
+  if (slab <= 0 || t <= slab || t % slab != 0)
+    return 1;
+  return t / slab;
+}
+
+size_t c2c_span_bytes(const H *h, const Plan &p) {
+  const long long e = static_cast<long long>(p.len - 1) * p.stride +
+                      (p.batch - 1) * p.dist + 1;
+  return static_cast<size_t>(e) * h->csize();
+}
+
+size_t real_span_bytes(const H *h, const Plan &p) {
+  // reals touched: input (len-1)*stride+1, complex output 2*(len/2)*stride+2
+  const long long in_r = static_cast<long long>(p.len - 1) * p.stride + 1;
+  const long long out_r = 2LL * (p.len / 2) * p.stride + 2;
+  const long long e = (p.batch - 1) * p.dist + std::max(in_r, out_r);
+  return static_cast<size_t>(e) * h->rsize;
+}
+
+bool overlaps(const char *a, size_t na, const char *b, size_t nb) {
+  return a < b + nb && b < a + na;
+}
+
+int issue_copy(H *h, void *dst, const void *src, size_t bytes) {
+  if (bytes == 0 || dst == src)
+    return B200FFT_SUCCESS;
+  h->stats.copies_issued++;
+  h->stats.bytes_copied += bytes;
+  b200fft_launch_record r{};
+  r.kind = 3;
+  r.stage = -1;
+  r.family = -1;
+  r.bytes = static_cast<long long>(bytes);
+  if (h->record_only) {
+    push_log(h, r);
+    return B200FFT_SUCCESS;
+  }
+  ProfileScope ps(h);
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, h->stream);
+  push_log(h, r);
+  ps.done();
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaMemcpyAsync");
+  return B200FFT_SUCCESS;
+}
+
+int flush_copy(H *h) {
+  if (!h->copy.active)
+    return B200FFT_SUCCESS;
+  h->copy.active = false;
+  return issue_copy(h, h->copy.dst, h->copy.src, h->copy.bytes);
+}
+
+// After a transform consumed [out0, out0+covered) of a held copy, move the
+// parts of the copy it did not cover.
+int finish_fused_copy(H *h, const char *out0, size_t covered) {
+  HeldCopy c = h->copy;
+  h->copy.active = false;
+  h->stats.fused_copies++;
+  const size_t pre = static_cast<size_t>(out0 - c.dst);
+  B2_TRY(issue_copy(h, c.dst, c.src, pre));
+  const size_t end = pre + covered;
+  if (end < c.bytes)
+    B2_TRY(issue_copy(h, c.dst + end, c.src + end, c.bytes - end));
+  return B200FFT_SUCCESS;
+}
+
+// Launch one pass of plan p. `in`/`out` point at the first transform;
+// slabs/slab (complex elements) describe a coalesced middle-axis run.
+int launch_pass(H *h, const Plan &p, int dir, const void *in, void *out,
+                long long slabs, long long slab, bool fused, int stage) {
+  const void *tw = nullptr;
+  B2_TRY(get_table(h, p.ch.tlen, &tw));
+  PassArgs a{};
+  a.in = in;
+  a.out = out;
+  a.tw = tw;
+  a.batch = p.batch;
+  a.total = p.batch * slabs;
+  long long bytes = 0;
+  const long long cs = static_cast<long long>(h->csize());
+  const long long rs = h->rsize;
+  if (p.kind == KIND_C2C) {
+    a.idist = a.odist = p.dist;
+    a.istride = a.ostride = p.stride;
+    a.islab = a.oslab = slab;
+    bytes = 2LL * a.total * p.len * cs;
+  } else {
+    const long long nc = p.len / 2 + 1;
+    bytes = a.total * (p.len * rs + nc * cs);
+    if (p.ch.family == 0) { // both sides complex units, contiguous rows
+      a.idist = a.odist = p.dist / 2;
+      a.istride = a.ostride = 1;
+      a.islab = a.oslab = 0;
+    } else if (p.kind == KIND_R2C) {
+      a.idist = p.dist;
+      a.istride = p.stride;
+      a.odist = p.dist / 2;
+      a.ostride = p.stride;
+    } else {
+      a.idist = p.dist / 2;
+      a.istride = p.stride;
+      a.odist = p.dist;
+      a.ostride = p.stride;
+    }
+  }
+  h->stats.kernel_launches++;
+  h->stats.bytes_transformed += static_cast<uint64_t>(bytes);
+  b200fft_launch_record r{};
+  r.kind = p.kind;
+  r.direction = dir;
+  r.stage = stage;
+  r.family = p.ch.family;
+  r.length = p.len;
+  r.fused_copy = fused ? 1 : 0;
+  r.transforms = a.total;
+  r.slabs = slabs;
+  r.bytes = bytes;
+  if (h->record_only || a.total == 0) {
+    push_log(h, r);
+    return B200FFT_SUCCESS;
+  }
+  ProfileScope ps(h);
+
+  const bool f64 = h->prec == B200FFT_F64;
+  const bool fwd = dir == B200FFT_FORWARD;
+  cudaError_t e;
+  if (p.ch.family == 0) {
+    if (p.kind == KIND_C2C)
+      e = f64 ? launch_static_c2c_f64(p.ch.L, p.ch.col, fwd, a, h->stream)
+              : launch_static_c2c_f32(p.ch.L, p.ch.col, fwd, a, h->stream);
+    else if (p.kind == KIND_R2C)
+      e = f64 ? launch_static_r2c_f64(p.ch.L, a, h->stream)
+              : launch_static_r2c_f32(p.ch.L, a, h->stream);
+    else
+      e = f64 ? launch_static_c2r_f64(p.ch.L, a, h->stream)
+              : launch_static_c2r_f32(p.ch.L, a, h->stream);
+  } else {
+    GenArgs g = p.ch.gen;
+    g.p = a;
+    e = launch_generic(f64, p.kind, p.ch.col, fwd, g, h->stream);
+  }
+  push_log(h, r);
+  ps.done();
+  if (e != cudaSuccess)
+    return cuda_fail(e, "transform kernel launch");
+  return B200FFT_SUCCESS;
+}
+
+int flush_run(H *h) {
+  if (!h->run.active)
+    return B200FFT_SUCCESS;
+  HeldRun r = h->run;
+  h->run.active = false;
+  const Plan &p = h->stages[r.stage];
+  const char *in = r.out0;
+  if (r.fused)
+    in = h->copy.src + (r.out0 - h->copy.dst);
+  const long long slab = r.lead > 1 ? static_cast<long long>(r.slab_bytes / h->csize()) : 0;
+  B2_TRY(launch_pass(h, p, r.dir, in, r.out0, r.count, slab, r.fused, r.stage));
+  if (r.fused)
+    B2_TRY(finish_fused_copy(h, r.out0, static_cast<size_t>(r.count) * r.slab_bytes));
+  return B200FFT_SUCCESS;
+}
+
+int flush_all(H *h) {
+  B2_TRY(flush_run(h));
+  return flush_copy(h);
+}
+
+bool copy_covers(const H *h, const char *p, size_t n) {
+  const HeldCopy &c = h->copy;
+  return c.active && p >= c.dst && p + n <= c.dst + c.bytes;
+}
+
+int check_handle(H *h) {
+  if (h == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft: null handle");
+  return B200FFT_SUCCESS;
+}
+
+bool is_device_ptr(const void *p) {
+  cudaPointerAttributes at{};
+  cudaError_t e = cudaPointerGetAttributes(&at, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice;
+}
+
+int make_plan(H *h, Plan *dst, int kind, int length, size_t batch,
+              ptrdiff_t stride, ptrdiff_t dist) {
+  if (length < 1)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft: length must be >= 1");
+  if (batch < 1 || stride < 1 || dist < 1)
+    return fail(B200FFT_ERR_INVALID_ARG,
+                "b200fft: batch, stride and dist must be >= 1");
+  if (batch > (1ull << 40) || stride > (1ll << 44) || dist > (1ll << 44))
+    return fail(B200FFT_ERR_RANGE, "b200fft: plan arguments exceed the supported range");
+  if (kind != KIND_C2C && batch > 1 &&
+      dist < 2LL * ((length / 2) * static_cast<long long>(stride) + 1))
+    return fail(B200FFT_ERR_INVALID_ARG,
+                "b200fft: in-place R2C/C2R rows overlap: dist must be at least "
+                "2*((length/2)*stride+1) reals");
+  B2_TRY(flush_all(h));
+  Plan p;
+  p.kind = kind;
+  p.len = length;
+  p.batch = static_cast<long long>(batch);
+  p.stride = stride;
+  p.dist = dist;
+  B2_TRY(choose_kernel(h->prec, kind, length, p.batch, stride, dist,
+                       h->force_generic, &p.ch));
+  const void *tw = nullptr;
+  B2_TRY(get_table(h, p.ch.tlen, &tw));
+  p.valid = true;
+  *dst = p;
+  return B200FFT_SUCCESS;
+}
+
+int exec_real(H *h, Plan &p, int kind, void *ptr) {
+  if (ptr == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft: null data pointer");
+  if (!p.valid)
+    return fail(B200FFT_ERR_NO_PLAN, kind == KIND_R2C
+                                         ? "b200fft: execute_r2c_inplace before create_r2c_inplace_plan"
+                                         : "b200fft: execute_c2r_inplace before create_c2r_inplace_plan");
+  h->stats.exec_calls++;
+  B2_TRY(flush_run(h));
+  char *cp = static_cast<char *>(ptr);
+  const size_t span = real_span_bytes(h, p);
+  bool fused = false;
+  if (h->copy.active) {
+    if (copy_covers(h, cp, span))
+      fused = true;
+    else
+      B2_TRY(flush_copy(h));
+  }
+  const void *in = fused ? static_cast<const void *>(h->copy.src + (cp - h->copy.dst)) : ptr;
+  const int dir = kind == KIND_R2C ? B200FFT_FORWARD : B200FFT_BACKWARD;
+  B2_TRY(launch_pass(h, p, dir, in, ptr, 1, 0, fused, -1));
+  if (fused)
+    B2_TRY(finish_fused_copy(h, cp, span));
+  return B200FFT_SUCCESS;
+}
+
+void *record_alloc(size_t bytes) {
+  void *p = nullptr;
+  if (posix_memalign(&p, 256, bytes ? bytes : 1) != 0)
+    return nullptr;
+  return p; // pages stay untouched: record-only handles never move data
+}
+
+} // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char *b200fft_last_error(void) { return g_err.c_str(); }
+
+int b200fft_version(void) { return 100; }
+
+int b200fft_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int b200fft_create(int precision, int num_stages, int plan_flag, unsigned flags,
+                   b200fft_handle *out) {
+  if (out == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_create: null output");
+  *out = nullptr;
+  if (precision != B200FFT_F32 && precision != B200FFT_F64)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_create: precision must be B200FFT_F32 or B200FFT_F64");
+  if (num_stages < 0 || num_stages > 64)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_create: num_stages out of range");
+  if (plan_flag < B200FFT_PLAN_ESTIMATE || plan_flag > B200FFT_PLAN_PATIENT)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_create: unknown plan flag");
+  if (env_flag("B200FFT_RECORD_ONLY"))
+    flags |= B200FFT_FLAG_RECORD_ONLY;
+  if (env_flag("B200FFT_NO_DEFER"))
+    flags |= B200FFT_FLAG_NO_DEFER;
+  if (env_flag("B200FFT_GENERIC_ONLY"))
+    flags |= B200FFT_FLAG_GENERIC_ONLY;
+  H *h = new H();
+  h->prec = precision;
+  h->rsize = precision == B200FFT_F64 ? 8 : 4;
+  h->nstages = num_stages;
+  h->plan_flag = plan_flag;
+  h->flags = flags;
+  h->record_only = (flags & B200FFT_FLAG_RECORD_ONLY) != 0;
+  h->defer = (flags & B200FFT_FLAG_NO_DEFER) == 0;
+  h->force_generic = (flags & B200FFT_FLAG_GENERIC_ONLY) != 0;
+  h->stages.resize(num_stages);
+  if (!h->record_only) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+      cudaGetLastError();
+      delete h;
+      return fail(B200FFT_ERR_NO_DEVICE,
+                  "b200fft_create: no CUDA device is visible; the B200 backend has no CPU path");
+    }
+    cudaGetDevice(&h->device);
+    cudaError_t e = cudaStreamCreate(&h->own);
+    if (e != cudaSuccess) {
+      delete h;
+      return cuda_fail(e, "cudaStreamCreate");
+    }
+    h->stream = h->own;
+  }
+  *out = h;
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_destroy(b200fft_handle h) {
+  if (h == nullptr)
+    return B200FFT_SUCCESS;
+  int rc = flush_all(h);
+  if (!h->record_only) {
+    if (h->stream)
+      cudaStreamSynchronize(h->stream);
+    resolve_timings(h);
+    for (cudaEvent_t e : h->event_pool)
+      cudaEventDestroy(e);
+    for (auto &kv : h->tables)
+      cudaFree(kv.second);
+    if (h->own)
+      cudaStreamDestroy(h->own);
+  }
+  delete h;
+  return rc;
+}
+
+int b200fft_set_stream(b200fft_handle h, void *cuda_stream) {
+  B2_TRY(check_handle(h));
+  B2_TRY(flush_all(h));
+  h->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : h->own;
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_plan_c2c(b200fft_handle h, int stage, int length, size_t batch,
+                     ptrdiff_t stride, ptrdiff_t dist) {
+  B2_TRY(check_handle(h));
+  if (stage < 0 || stage >= h->nstages)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_plan_c2c: stage " + std::to_string(stage) +
+                                             " outside [0, num_stages)");
+  return make_plan(h, &h->stages[stage], KIND_C2C, length, batch, stride, dist);
+}
+
+int b200fft_exec_c2c(b200fft_handle h, int stage, int direction, void *data) {
+  B2_TRY(check_handle(h));
+  if (stage < 0 || stage >= h->nstages)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_exec_c2c: stage out of range");
+  if (direction != B200FFT_FORWARD && direction != B200FFT_BACKWARD)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_exec_c2c: bad direction");
+  if (data == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_exec_c2c: null data pointer");
+  Plan &p = h->stages[stage];
+  if (!p.valid)
+    return fail(B200FFT_ERR_NO_PLAN, "b200fft_exec_c2c: stage " + std::to_string(stage) +
+                                         " has no plan");
+  h->stats.exec_calls++;
+  char *cp = static_cast<char *>(data);
+  HeldRun &r = h->run;
+  if (r.active && r.stage == stage && r.dir == direction && r.count < r.lead &&
+      cp == r.out0 + static_cast<size_t>(r.count) * r.slab_bytes) {
+    r.count++;
+    h->stats.coalesced_calls++;
+    if (r.count == r.lead)
+      return flush_run(h);
+    return B200FFT_SUCCESS;
+  }
+  B2_TRY(flush_run(h));
+  const long long lead = infer_lead(h, p);
+  const size_t slab_bytes = lead > 1 ? static_cast<size_t>(p.len) * p.batch * h->csize()
+                                     : c2c_span_bytes(h, p);
+  const size_t region = static_cast<size_t>(lead) * slab_bytes;
+  bool fused = false;
+  if (h->copy.active) {
+    if (copy_covers(h, cp, region))
+      fused = true;
+    else
+      B2_TRY(flush_copy(h));
+  }
+  r.active = true;
+  r.stage = stage;
+  r.dir = direction;
+  r.out0 = cp;
+  r.count = 1;
+  r.lead = lead;
+  r.slab_bytes = slab_bytes;
+  r.fused = fused;
+  if (lead == 1)
+    return flush_run(h);
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_plan_r2c(b200fft_handle h, int length, size_t batch,
+                     ptrdiff_t stride, ptrdiff_t dist) {
+  B2_TRY(check_handle(h));
+  return make_plan(h, &h->r2c, KIND_R2C, length, batch, stride, dist);
+}
+
+int b200fft_exec_r2c(b200fft_handle h, void *padded_real) {
+  B2_TRY(check_handle(h));
+  return exec_real(h, h->r2c, KIND_R2C, padded_real);
+}
+
+int b200fft_plan_c2r(b200fft_handle h, int length, size_t batch,
+                     ptrdiff_t stride, ptrdiff_t dist) {
+  B2_TRY(check_handle(h));
+  return make_plan(h, &h->c2r, KIND_C2R, length, batch, stride, dist);
+}
+
+int b200fft_exec_c2r(b200fft_handle h, void *padded_real) {
+  B2_TRY(check_handle(h));
+  return exec_real(h, h->c2r, KIND_C2R, padded_real);
+}
+
+int b200fft_memcpy(b200fft_handle h, void *dst, const void *src, size_t bytes) {
+  B2_TRY(check_handle(h));
+  h->stats.memcpy_calls++;
+  B2_TRY(flush_all(h));
+  if (bytes == 0 || dst == src)
+    return B200FFT_SUCCESS;
+  if (dst == nullptr || src == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_memcpy: null pointer");
+  const char *s = static_cast<const char *>(src);
+  char *d = static_cast<char *>(dst);
+  const bool hold = h->defer && !overlaps(d, bytes, s, bytes) &&
+                    (h->record_only || (is_device_ptr(dst) && is_device_ptr(src)));
+  if (hold) {
+    h->copy.active = true;
+    h->copy.dst = d;
+    h->copy.src = s;
+    h->copy.bytes = bytes;
+    return B200FFT_SUCCESS;
+  }
+  return issue_copy(h, dst, src, bytes);
+}
+
+int b200fft_memcpy2d(b200fft_handle h, void *dst, size_t dpitch, const void *src,
+                     size_t spitch, size_t width, size_t height) {
+  B2_TRY(check_handle(h));
+  h->stats.memcpy_calls++;
+  B2_TRY(flush_all(h));
+  if (width == 0 || height == 0)
+    return B200FFT_SUCCESS;
+  h->stats.copies_issued++;
+  h->stats.bytes_copied += width * height;
+  b200fft_launch_record r{};
+  r.kind = 3;
+  r.stage = -1;
+  r.family = -1;
+  r.bytes = static_cast<long long>(width * height);
+  if (h->record_only) {
+    push_log(h, r);
+    return B200FFT_SUCCESS;
+  }
+  ProfileScope ps(h);
+  cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height,
+                                    cudaMemcpyDefault, h->stream);
+  push_log(h, r);
+  ps.done();
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaMemcpy2DAsync");
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_flush(b200fft_handle h) {
+  B2_TRY(check_handle(h));
+  return flush_all(h);
+}
+
+int b200fft_sync(b200fft_handle h) {
+  B2_TRY(check_handle(h));
+  B2_TRY(flush_all(h));
+  if (h->record_only)
+    return B200FFT_SUCCESS;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaStreamSynchronize");
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_alloc(size_t bytes, void **ptr) {
+  if (ptr == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_alloc: null output");
+  *ptr = nullptr;
+  if (bytes == 0)
+    return B200FFT_SUCCESS;
+  if (env_flag("B200FFT_RECORD_ONLY")) {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    *ptr = record_alloc(bytes);
+    return *ptr ? B200FFT_SUCCESS : fail(B200FFT_ERR_RANGE, "b200fft_alloc: host allocation failed");
+  }
+  cudaError_t e = cudaMalloc(ptr, bytes);
+  if (e != cudaSuccess) {
+    *ptr = nullptr;
+    return cuda_fail(e, "cudaMalloc");
+  }
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_free(void *ptr) {
+  if (ptr == nullptr)
+    return B200FFT_SUCCESS;
+  if (env_flag("B200FFT_RECORD_ONLY")) {
+    std::free(ptr);
+    return B200FFT_SUCCESS;
+  }
+  cudaError_t e = cudaFree(ptr);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaFree");
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_set_profiling(b200fft_handle h, int on) {
+  B2_TRY(check_handle(h));
+  B2_TRY(flush_all(h));
+  h->profiling = on != 0;
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_get_stats(b200fft_handle h, b200fft_stats *out) {
+  B2_TRY(check_handle(h));
+  if (out == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_get_stats: null output");
+  *out = h->stats;
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_reset_stats(b200fft_handle h) {
+  B2_TRY(check_handle(h));
+  if (!h->record_only)
+    resolve_timings(h);
+  h->stats = b200fft_stats{};
+  h->log_base += h->log.size();
+  h->log.clear();
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_get_log(b200fft_handle h, b200fft_launch_record *out, int cap,
+                    int *count) {
+  B2_TRY(check_handle(h));
+  if (count == nullptr || (cap > 0 && out == nullptr))
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_get_log: null output");
+  B2_TRY(flush_all(h));
+  if (!h->record_only)
+    resolve_timings(h);
+  const int n = std::min<int>(cap, static_cast<int>(h->log.size()));
+  const int start = static_cast<int>(h->log.size()) - n;
+  for (int i = 0; i < n; ++i)
+    out[i] = h->log[start + i];
+  *count = n;
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_describe(int precision, int kind, int length, size_t batch,
+                     ptrdiff_t stride, ptrdiff_t dist, char *buf, size_t buflen) {
+  if (buf == nullptr || buflen == 0)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_describe: null buffer");
+  if (kind < 0 || kind > 2 || length < 1 || batch < 1 || stride < 1 || dist < 1)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_describe: bad arguments");
+  Choice ch;
+  B2_TRY(choose_kernel(precision, kind, length, static_cast<long long>(batch), stride,
+                       dist, false, &ch));
+  std::string s = describe_choice(ch, kind);
+  std::snprintf(buf, buflen, "%s", s.c_str());
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_supported(int precision, int kind, int length) {
+  if (length < 1 || kind < 0 || kind > 2)
+    return 0;
+  Choice ch;
+  std::string keep = g_err;
+  const int rc = choose_kernel(precision, kind, length, 1, 1, kind == KIND_C2C ? length : 2 * (length / 2 + 1), false, &ch);
+  g_err = keep;
+  return rc == B200FFT_SUCCESS ? 1 : 0;
+}
+
+} // extern "C"

@@ -1,0 +1,168 @@
+// Host+device shared definitions of the B200 transform engine: launch
+// arguments, kernel configuration rules and the radix schedule.
+//
+// A "pass" is one batched 1D transform along one axis of a ParaFaFT stage
+// buffer. Transform b of a pass starts at element
+//     (b / batch) * slab + (b % batch) * dist
+// and its points sit `stride` elements apart. `batch`, `dist` and `stride` are
+// the plan arguments of Backend::create_stage_plan
+// (backend/fft_backend.hpp:83-93); `slab` is the pointer step between the
+// consecutive execute_stage calls that ParaFaFT issues for a middle axis
+// (parafaft_c2c.hpp:875-896, parafaft_r2c.hpp:1224-1244), which one pass
+// covers at once.
+#pragma once
+
+#include <stddef.h>
+#include <stdint.h>
+
+namespace b200fft {
+
+enum : int { KIND_C2C = 0, KIND_R2C = 1, KIND_C2R = 2 };
+
+// Launch arguments shared by all transform kernels. Input and output sides
+// carry their own element units: complex elements for C2C; for R2C the input
+// side is in reals and the output side in complex elements; for C2R the
+// reverse. The specialised R2C/C2R kernels take both sides in complex units.
+struct PassArgs {
+  const void *in;
+  void *out;
+  const void *tw;     // twiddle table exp(-2*pi*i*m/tlen), m in [0, tlen)
+  long long total;    // transforms in the launch (batch * slabs)
+  long long batch;    // transforms per slab
+  long long idist, istride, islab;
+  long long odist, ostride, oslab;
+};
+
+// Division by a runtime constant d < 2^31 for dividends n < 2^31:
+//   q = (n * m) >> (32 + s)  with  m = ceil(2^(31 + l) / d),  l = ceil(log2 d),
+// s = l - 1 (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994). d == 1 is encoded as m == 0.
+struct FastDiv {
+  uint32_t m;
+  uint32_t s;
+  uint32_t d;
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f{0u, 0u, d};
+  if (d <= 1)
+    return f;
+  uint32_t l = 0;
+  while ((1ull << l) < d)
+    ++l;
+  const unsigned long long num = (1ull << (31 + l)) + d - 1;
+  f.m = static_cast<uint32_t>(num / d);
+  f.s = l - 1;
+  return f;
+}
+
+// Runtime-generic kernel limits.
+constexpr int kGenMaxStages = 24;
+constexpr int kGenMaxPrime = 61; // largest prime radix done by direct DFT
+constexpr int kGenThreads = 256;
+
+struct GenArgs {
+  PassArgs p;
+  int L;       // complex points per transform handled by the stage loop
+  int nreal;   // real length for R2C/C2R (0 for C2C)
+  int lout;    // outputs per transform written by the store loop
+  int nst;     // number of radix stages
+  int TB;      // transforms per CTA (power of two)
+  int logTB;
+  int tscale;  // table index = exponent * tscale
+  int odd;     // R2C/C2R of odd real length (full-length complex transform)
+  int rad[kGenMaxStages];
+  int nsv[kGenMaxStages];
+  FastDiv ns[kGenMaxStages];  // divide by Ns (product of earlier radices)
+  FastDiv bq[kGenMaxStages];  // divide by L / radix
+  FastDiv Ldiv;               // divide by L
+  FastDiv Loutdiv;            // divide by lout
+};
+
+// ---- compile-time radix schedule for the specialised kernels ------------
+// Radix order: 8s, then one 4 or 2, then 5s, then 3s. Stockham stage s with
+// radix R reads points j + r*L/R and writes (j/Ns)*Ns*R + j%Ns + r*Ns,
+// Ns = product of the radices before s, so the last stage writes natural
+// order directly.
+template <int L> struct SchedS {
+  int nst = 0;
+  int rad[24] = {};
+  int ns[24] = {};
+  int rest = 1;
+  constexpr SchedS() {
+    int m = L;
+    int k = 0;
+    while (m % 8 == 0 && m > 1) {
+      rad[k++] = 8;
+      m /= 8;
+    }
+    if (m % 4 == 0) {
+      rad[k++] = 4;
+      m /= 4;
+    }
+    if (m % 2 == 0) {
+      rad[k++] = 2;
+      m /= 2;
+    }
+    while (m % 5 == 0) {
+      rad[k++] = 5;
+      m /= 5;
+    }
+    while (m % 3 == 0) {
+      rad[k++] = 3;
+      m /= 3;
+    }
+    rest = m;
+    nst = k;
+    int p = 1;
+    for (int i = 0; i < k; ++i) {
+      ns[i] = p;
+      p *= rad[i];
+    }
+  }
+};
+
+// Configuration of a specialised kernel: NT threads, TB transforms per CTA,
+// P = NT/TB threads per transform, E points per thread.
+//  * column layout (points strided, neighbouring transforms adjacent in
+//    memory): a CTA owns TB adjacent transforms so every point row it loads is
+//    a contiguous TB-element segment; target tile 8192 (f32) / 4096 (f64)
+//    points, at most 32 / 16 points per thread.
+//  * row layout (points contiguous): P threads per transform read contiguous
+//    runs; E between 8 and 32 (f32) / 16 (f64).
+struct CfgS {
+  int NT, TB, P, E;
+};
+
+constexpr int ce_min(int a, int b) { return a < b ? a : b; }
+constexpr int ce_max(int a, int b) { return a > b ? a : b; }
+
+constexpr CfgS cfg_static(int esize, int L, bool col) {
+  const int NT = 256;
+  const int target = esize == 8 ? 8192 : 4096; // esize = sizeof(complex)
+  const int emax = esize == 8 ? 32 : 16;
+  if (col) {
+    int TB = ce_min(NT, ce_max(1, target / L));
+    int P = NT / TB;
+    int E = (TB * L) / NT;
+    if (E < 1)
+      E = 1;
+    return CfgS{NT, TB, P, E};
+  }
+  int E = L / 32;
+  if (E < 8)
+    E = ce_min(8, L);
+  if (E > emax)
+    E = emax;
+  int P = L / E;
+  int TB = NT / P;
+  return CfgS{NT, TB, P, E};
+}
+
+constexpr bool is_pow2(long long x) { return x > 0 && (x & (x - 1)) == 0; }
+
+// Lengths with a specialised kernel (complex points of the stage loop).
+constexpr int kStaticMaxL = 4096;
+constexpr bool static_length_ok(int L) { return L >= 2 && L <= kStaticMaxL && is_pow2(L); }
+
+} // namespace b200fft

@@ -1,0 +1,562 @@
+// Device code of the B200 transform engine.
+//
+// Every transform is a Stockham autosort FFT over shared memory:
+//   stage s, radix R, Ns = product of earlier radices, butterfly j < L/R:
+//     read   x_r = a[j + r*L/R]                       (r < R)
+//     twiddle x_r *= w^(r*(j mod Ns)),  w = exp(-+2*pi*i/(Ns*R))
+//     DFT_R over (x_0..x_{R-1})
+//     write  b[(j/Ns)*Ns*R + (j mod Ns) + r*Ns] = X_r
+// The first stage reads global memory directly and the last stage writes it
+// directly (its write index reduces to j + r*L/R), so a transform costs one
+// HBM read and one HBM write plus (stages-1) shared-memory exchanges.
+// Twiddles come from a table exp(-2*pi*i*m/tlen) generated once per length in
+// FP64 by sincospi after exact integer reduction of m (twiddle_table_kernel),
+// then rounded to the working precision.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_common.hpp"
+
+namespace b200fft {
+
+#define BF_D __device__ __forceinline__
+
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
+template <typename T> using cvec = typename Vec2<T>::type;
+
+BF_D float2 cmake(float x, float y) { return make_float2(x, y); }
+BF_D double2 cmake(double x, double y) { return make_double2(x, y); }
+template <typename V> BF_D V czero() { V r; r.x = 0; r.y = 0; return r; }
+template <typename V> BF_D V cadd(V a, V b) { return cmake(a.x + b.x, a.y + b.y); }
+template <typename V> BF_D V csub(V a, V b) { return cmake(a.x - b.x, a.y - b.y); }
+template <typename V> BF_D V cconj(V a) { return cmake(a.x, -a.y); }
+// a * w, or a * conj(w) when CONJ
+template <bool CONJ, typename V> BF_D V cmulw(V a, V w) {
+  if (CONJ)
+    return cmake(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+  return cmake(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+}
+// multiply by -i (forward) or +i (backward)
+template <bool FWD, typename V> BF_D V rot(V a) {
+  return FWD ? cmake(a.y, -a.x) : cmake(-a.y, a.x);
+}
+
+BF_D uint32_t fdiv(uint32_t n, const FastDiv &f) {
+  return f.m == 0 ? n : (__umulhi(n, f.m) >> f.s);
+}
+
+// ---- small DFTs (natural order in and out) -------------------------------
+template <bool FWD, typename V> BF_D void dft2(V &a, V &b) {
+  V t = csub(a, b);
+  a = cadd(a, b);
+  b = t;
+}
+
+template <bool FWD, typename V> BF_D void dft3(V *v) {
+  using T = decltype(v[0].x);
+  const T s = T(0.86602540378443864676372317075294);
+  V t = cadd(v[1], v[2]);
+  V d = csub(v[1], v[2]);
+  V m = cmake(v[0].x - T(0.5) * t.x, v[0].y - T(0.5) * t.y);
+  V sd = rot<FWD>(cmake(s * d.x, s * d.y)); // -+ i*s*d
+  v[0] = cadd(v[0], t);
+  v[1] = cadd(m, sd);
+  v[2] = csub(m, sd);
+}
+
+template <bool FWD, typename V> BF_D void dft4(V &a0, V &a1, V &a2, V &a3) {
+  V t0 = cadd(a0, a2), t1 = csub(a0, a2);
+  V t2 = cadd(a1, a3), t3 = rot<FWD>(csub(a1, a3));
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  a1 = cadd(t1, t3);
+  a3 = csub(t1, t3);
+}
+
+template <bool FWD, typename V> BF_D void dft5(V *v) {
+  using T = decltype(v[0].x);
+  const T c1 = T(0.30901699437494742410229341718282);
+  const T c2 = T(-0.80901699437494742410229341718282);
+  const T s1 = T(0.95105651629515357211643933337938);
+  const T s2 = T(0.58778525229247312916870595463907);
+  V a = cadd(v[1], v[4]), b = csub(v[1], v[4]);
+  V c = cadd(v[2], v[3]), d = csub(v[2], v[3]);
+  V m1 = cmake(v[0].x + c1 * a.x + c2 * c.x, v[0].y + c1 * a.y + c2 * c.y);
+  V m2 = cmake(v[0].x + c2 * a.x + c1 * c.x, v[0].y + c2 * a.y + c1 * c.y);
+  V n1 = rot<FWD>(cmake(s1 * b.x + s2 * d.x, s1 * b.y + s2 * d.y));
+  V n2 = rot<FWD>(cmake(s2 * b.x - s1 * d.x, s2 * b.y - s1 * d.y));
+  v[0] = cmake(v[0].x + a.x + c.x, v[0].y + a.y + c.y);
+  v[1] = cadd(m1, n1);
+  v[4] = csub(m1, n1);
+  v[2] = cadd(m2, n2);
+  v[3] = csub(m2, n2);
+}
+
+template <bool FWD, typename V> BF_D void dft8(V *v) {
+  using T = decltype(v[0].x);
+  const T h = T(0.70710678118654752440084436210485);
+  V e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  V o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4<FWD>(e0, e1, e2, e3);
+  dft4<FWD>(o0, o1, o2, o3);
+  // o_k *= w8^k, w8 = exp(-+ i*pi/4)
+  if (FWD) {
+    o1 = cmake(h * (o1.x + o1.y), h * (o1.y - o1.x));
+    o3 = cmake(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+  } else {
+    o1 = cmake(h * (o1.x - o1.y), h * (o1.x + o1.y));
+    o3 = cmake(-h * (o3.x + o3.y), h * (o3.x - o3.y));
+  }
+  o2 = rot<FWD>(o2);
+  v[0] = cadd(e0, o0);
+  v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1);
+  v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2);
+  v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3);
+  v[7] = csub(e3, o3);
+}
+
+template <int R, bool FWD, typename V> BF_D void dft(V *v) {
+  if constexpr (R == 1) {
+  } else if constexpr (R == 2) {
+    dft2<FWD>(v[0], v[1]);
+  } else if constexpr (R == 3) {
+    dft3<FWD>(v);
+  } else if constexpr (R == 4) {
+    dft4<FWD>(v[0], v[1], v[2], v[3]);
+  } else if constexpr (R == 5) {
+    dft5<FWD>(v);
+  } else if constexpr (R == 8) {
+    dft8<FWD>(v);
+  } else {
+    static_assert(R == 0, "unsupported radix");
+  }
+}
+
+template <typename V> BF_D V ldtw(const V *tw, int m) { return __ldg(tw + m); }
+
+// ==========================================================================
+// Family S: lengths known at compile time (powers of two up to 4096).
+// ==========================================================================
+template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND>
+struct KS {
+  using V = cvec<T>;
+  static constexpr SchedS<L> S{};
+  static constexpr int NST = S.nst;
+  static constexpr int P = NT / TB; // threads per transform
+  static constexpr int LP = COL ? L : (L + L / 8);
+  static constexpr int TSCALE = (KIND == KIND_C2C) ? 1 : 2;
+  static constexpr bool WARP_SYNC = !COL && (P <= 32) && (32 % P == 0);
+  static_assert(NT % TB == 0, "TB must divide NT");
+  static_assert(S.rest == 1, "length not factorable");
+
+  static constexpr int emax() {
+    int e = 1;
+    for (int s = 0; s < S.nst; ++s) {
+      int B = L / S.rad[s];
+      int K = (B + P - 1) / P;
+      if (K * S.rad[s] > e)
+        e = K * S.rad[s];
+    }
+    return e;
+  }
+  static constexpr int EMAX = emax();
+
+  static constexpr size_t smem_bytes() {
+    return static_cast<size_t>(TB) * LP * sizeof(V);
+  }
+
+  struct Ctx {
+    int g, tb;
+    bool act;
+    const V *gin;
+    V *gout;
+    const V *tw;
+    long long ist, ost;
+    V *sm;
+  };
+
+  static BF_D void bar() {
+    if constexpr (WARP_SYNC)
+      __syncwarp();
+    else
+      __syncthreads();
+  }
+  static BF_D int sidx(const Ctx &c, int n) {
+    if constexpr (COL)
+      return n * TB + c.tb;
+    else
+      return c.tb * LP + n + (n >> 3);
+  }
+
+  // C2R input: Z[n] = E + i*O from X[n] and X[L-n] (real length 2L).
+  static BF_D V c2r_pre(const Ctx &c, int n) {
+    V xa = c.gin[(long long)n * c.ist];
+    V xb = c.gin[(long long)(L - n) * c.ist];
+    if (n == 0) {
+      xa.y = T(0);
+      xb.y = T(0);
+    }
+    V e = cadd(xa, cconj(xb));
+    V o = cmulw<true>(csub(xa, cconj(xb)), ldtw(c.tw, n));
+    return cmake(e.x - o.y, e.y + o.x);
+  }
+
+  // R2C output k in [0, L] from Z held in shared memory (natural order).
+  static BF_D V r2c_post(const Ctx &c, int k) {
+    V a = c.sm[sidx(c, k == L ? 0 : k)];
+    V b = cconj(c.sm[sidx(c, k == 0 ? 0 : L - k)]);
+    V e = cmake(T(0.5) * (a.x + b.x), T(0.5) * (a.y + b.y));
+    V d = csub(a, b);
+    V o = cmake(T(0.5) * d.y, T(-0.5) * d.x); // -i*(a-b)/2
+    return cadd(e, cmulw<false>(o, ldtw(c.tw, k)));
+  }
+
+  template <int s> static BF_D void run(Ctx &c, V (&v)[EMAX]) {
+    constexpr int R = S.rad[s];
+    constexpr int Ns = S.ns[s];
+    constexpr int B = L / R;
+    constexpr int K = (B + P - 1) / P;
+    constexpr bool FULL = (B % P) == 0;
+    if constexpr (s > 0) {
+#pragma unroll
+      for (int i = 0; i < K; ++i) {
+        const int j = c.g + P * i;
+        if (FULL || j < B) {
+          const int k = j % Ns;
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            const int e = r * k * (L / (Ns * R));
+            v[i * R + r] = cmulw<!FWD>(v[i * R + r], ldtw(c.tw, e * TSCALE));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < K; ++i)
+      dft<R, FWD>(&v[i * R]);
+
+    if constexpr (s == NST - 1) {
+      if constexpr (KIND == KIND_R2C) {
+        if constexpr (s > 0)
+          bar();
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+          const int j = c.g + P * i;
+          if (FULL || j < B) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+              c.sm[sidx(c, j + r * B)] = v[i * R + r];
+          }
+        }
+        bar();
+        constexpr int KO = (L + 1 + P - 1) / P;
+#pragma unroll
+        for (int i = 0; i < KO; ++i) {
+          const int k = c.g + P * i;
+          if (c.act && k <= L)
+            c.gout[(long long)k * c.ost] = r2c_post(c, k);
+        }
+      } else {
+        if (c.act) {
+#pragma unroll
+          for (int i = 0; i < K; ++i) {
+            const int j = c.g + P * i;
+            if (FULL || j < B) {
+#pragma unroll
+              for (int r = 0; r < R; ++r)
+                c.gout[(long long)(j + r * B) * c.ost] = v[i * R + r];
+            }
+          }
+        }
+      }
+    } else {
+      if constexpr (s > 0)
+        bar();
+#pragma unroll
+      for (int i = 0; i < K; ++i) {
+        const int j = c.g + P * i;
+        if (FULL || j < B) {
+          const int base = (j / Ns) * Ns * R + (j % Ns);
+#pragma unroll
+          for (int r = 0; r < R; ++r)
+            c.sm[sidx(c, base + r * Ns)] = v[i * R + r];
+        }
+      }
+      bar();
+      constexpr int R2 = S.rad[s + 1];
+      constexpr int B2 = L / R2;
+      constexpr int K2 = (B2 + P - 1) / P;
+      constexpr bool FULL2 = (B2 % P) == 0;
+#pragma unroll
+      for (int i = 0; i < K2; ++i) {
+        const int j = c.g + P * i;
+        if (FULL2 || j < B2) {
+#pragma unroll
+          for (int r = 0; r < R2; ++r)
+            v[i * R2 + r] = c.sm[sidx(c, j + r * B2)];
+        }
+      }
+      run<s + 1>(c, v);
+    }
+  }
+
+  static BF_D void entry(const PassArgs &a, V *sm) {
+    Ctx c;
+    const int tid = threadIdx.x;
+    c.g = COL ? (tid / TB) : (tid % P);
+    c.tb = COL ? (tid % TB) : (tid / P);
+    const long long b = static_cast<long long>(blockIdx.x) * TB + c.tb;
+    c.act = b < a.total;
+    long long ioff = 0, ooff = 0;
+    if (c.act) {
+      const long long sl = b / a.batch;
+      const long long w = b - sl * a.batch;
+      ioff = sl * a.islab + w * a.idist;
+      ooff = sl * a.oslab + w * a.odist;
+    }
+    c.gin = reinterpret_cast<const V *>(a.in) + ioff;
+    c.gout = reinterpret_cast<V *>(a.out) + ooff;
+    c.tw = reinterpret_cast<const V *>(a.tw);
+    c.ist = a.istride;
+    c.ost = a.ostride;
+    c.sm = sm;
+
+    V v[EMAX];
+    constexpr int R = S.rad[0];
+    constexpr int B = L / R;
+    constexpr int K = (B + P - 1) / P;
+    constexpr bool FULL = (B % P) == 0;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      const int j = c.g + P * i;
+      const bool ok = c.act && (FULL || j < B);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int n = j + r * B;
+        if constexpr (KIND == KIND_C2R)
+          v[i * R + r] = ok ? c2r_pre(c, n) : czero<V>();
+        else
+          v[i * R + r] = ok ? c.gin[(long long)n * c.ist] : czero<V>();
+      }
+    }
+    run<0>(c, v);
+  }
+};
+
+template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND>
+__global__ void __launch_bounds__(NT)
+    fft_static_kernel(const PassArgs a) {
+  using K = KS<T, L, NT, TB, COL, FWD, KIND>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  K::entry(a, reinterpret_cast<typename K::V *>(smraw));
+}
+
+// ==========================================================================
+// Family G: runtime length and radix schedule (any length whose prime
+// factors are 2, 3, 5, 7 or another prime <= kGenMaxPrime).
+// ==========================================================================
+template <bool COL> BF_D int gidx(int tb, int n, int TB, int L) {
+  return COL ? n * TB + tb : tb * L + n;
+}
+
+template <int R, bool FWD, bool COL, typename V>
+BF_D void gen_butterfly(const GenArgs &a, const V *A, V *Bm, const V *tw,
+                        int tb, int j, int k, int Bq, int Ns, int texp) {
+  V v[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    v[r] = A[gidx<COL>(tb, j + r * Bq, a.TB, a.L)];
+    if (r > 0 && Ns > 1)
+      v[r] = cmulw<!FWD>(v[r], ldtw(tw, r * k * texp * a.tscale));
+  }
+  dft<R, FWD>(v);
+  const int base = (j - k) * R + k; // (j/Ns)*Ns*R + k
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+    Bm[gidx<COL>(tb, base + r * Ns, a.TB, a.L)] = v[r];
+}
+
+// Prime radix p by direct summation; DFT constants come from the table:
+// exp(-2*pi*i*r*m/p) = tw[((r*m) mod p) * (L/p) * tscale].
+template <bool FWD, bool COL, typename V>
+BF_D void gen_butterfly_prime(const GenArgs &a, const V *A, V *Bm, const V *tw,
+                              int p, int tb, int j, int k, int Bq, int Ns,
+                              int texp) {
+  V x[kGenMaxPrime];
+  for (int r = 0; r < p; ++r) {
+    V t = A[gidx<COL>(tb, j + r * Bq, a.TB, a.L)];
+    if (r > 0 && Ns > 1)
+      t = cmulw<!FWD>(t, ldtw(tw, r * k * texp * a.tscale));
+    x[r] = t;
+  }
+  const int step = (a.L / p) * a.tscale;
+  const int base = (j - k) * p + k;
+  for (int m = 0; m < p; ++m) {
+    V acc = x[0];
+    int e = 0;
+    for (int r = 1; r < p; ++r) {
+      e += m;
+      if (e >= p)
+        e -= p;
+      acc = cadd(acc, cmulw<!FWD>(x[r], ldtw(tw, e * step)));
+    }
+    Bm[gidx<COL>(tb, base + m * Ns, a.TB, a.L)] = acc;
+  }
+}
+
+template <typename T, bool COL, int KIND, bool FWD>
+__global__ void __launch_bounds__(kGenThreads) fft_generic_kernel(const GenArgs a) {
+  using V = cvec<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V *A = reinterpret_cast<V *>(smraw);
+  V *Bm = A + static_cast<size_t>(a.TB) * a.L;
+  const V *tw = reinterpret_cast<const V *>(a.p.tw);
+  const int tid = threadIdx.x;
+  const int TB = a.TB, L = a.L;
+  const long long tile0 = static_cast<long long>(blockIdx.x) * TB;
+
+  auto offsets = [&](int tb, long long &io, long long &oo) -> bool {
+    const long long b = tile0 + tb;
+    if (b >= a.p.total)
+      return false;
+    const long long sl = b / a.p.batch;
+    const long long w = b - sl * a.p.batch;
+    io = sl * a.p.islab + w * a.p.idist;
+    oo = sl * a.p.oslab + w * a.p.odist;
+    return true;
+  };
+
+  // ---- load ---------------------------------------------------------------
+  for (int e = tid; e < TB * L; e += kGenThreads) {
+    int tb, n;
+    if (COL) {
+      tb = e & (TB - 1);
+      n = e >> a.logTB;
+    } else {
+      tb = static_cast<int>(fdiv(static_cast<uint32_t>(e), a.Ldiv));
+      n = e - tb * L;
+    }
+    long long io, oo;
+    V val = czero<V>();
+    if (offsets(tb, io, oo)) {
+      const long long is = a.p.istride;
+      if constexpr (KIND == KIND_C2C) {
+        val = reinterpret_cast<const V *>(a.p.in)[io + n * is];
+      } else if constexpr (KIND == KIND_R2C) {
+        const T *x = reinterpret_cast<const T *>(a.p.in) + io;
+        if (a.odd)
+          val = cmake(x[n * is], T(0));
+        else
+          val = cmake(x[(2LL * n) * is], x[(2LL * n + 1) * is]);
+      } else { // C2R
+        const V *X = reinterpret_cast<const V *>(a.p.in) + io;
+        if (a.odd) {
+          const int nh = a.nreal / 2;
+          if (n <= nh) {
+            val = X[n * is];
+            if (n == 0)
+              val.y = T(0);
+          } else {
+            val = cconj(X[(long long)(a.nreal - n) * is]);
+          }
+        } else {
+          V xa = X[n * is];
+          V xb = X[(long long)(L - n) * is];
+          if (n == 0) {
+            xa.y = T(0);
+            xb.y = T(0);
+          }
+          V ev = cadd(xa, cconj(xb));
+          V ov = cmulw<true>(csub(xa, cconj(xb)), ldtw(tw, n));
+          val = cmake(ev.x - ov.y, ev.y + ov.x);
+        }
+      }
+    }
+    A[gidx<COL>(tb, n, TB, L)] = val;
+  }
+  __syncthreads();
+
+  // ---- stages ---------------------------------------------------------------
+  for (int s = 0; s < a.nst; ++s) {
+    const int R = a.rad[s];
+    const int Ns = a.nsv[s];
+    const int Bq = L / R;
+    const int texp = L / (Ns * R);
+    const int cnt = TB * Bq;
+    for (int q = tid; q < cnt; q += kGenThreads) {
+      int tb, j;
+      if (COL) {
+        tb = q & (TB - 1);
+        j = q >> a.logTB;
+      } else {
+        tb = static_cast<int>(fdiv(static_cast<uint32_t>(q), a.bq[s]));
+        j = q - tb * Bq;
+      }
+      const int k = j - static_cast<int>(fdiv(static_cast<uint32_t>(j), a.ns[s])) * Ns;
+      switch (R) {
+      case 2: gen_butterfly<2, FWD, COL>(a, A, Bm, tw, tb, j, k, Bq, Ns, texp); break;
+      case 3: gen_butterfly<3, FWD, COL>(a, A, Bm, tw, tb, j, k, Bq, Ns, texp); break;
+      case 4: gen_butterfly<4, FWD, COL>(a, A, Bm, tw, tb, j, k, Bq, Ns, texp); break;
+      case 5: gen_butterfly<5, FWD, COL>(a, A, Bm, tw, tb, j, k, Bq, Ns, texp); break;
+      case 8: gen_butterfly<8, FWD, COL>(a, A, Bm, tw, tb, j, k, Bq, Ns, texp); break;
+      default:
+        gen_butterfly_prime<FWD, COL>(a, A, Bm, tw, R, tb, j, k, Bq, Ns, texp);
+        break;
+      }
+    }
+    __syncthreads();
+    V *t = A;
+    A = Bm;
+    Bm = t;
+  }
+
+  // ---- store ----------------------------------------------------------------
+  const int lout = a.lout;
+  for (int e = tid; e < TB * lout; e += kGenThreads) {
+    int tb, k;
+    if (COL) {
+      tb = e & (TB - 1);
+      k = e >> a.logTB;
+    } else {
+      tb = static_cast<int>(fdiv(static_cast<uint32_t>(e), a.Loutdiv));
+      k = e - tb * lout;
+    }
+    long long io, oo;
+    if (!offsets(tb, io, oo))
+      continue;
+    const long long os = a.p.ostride;
+    if constexpr (KIND == KIND_C2C) {
+      reinterpret_cast<V *>(a.p.out)[oo + k * os] = A[gidx<COL>(tb, k, TB, L)];
+    } else if constexpr (KIND == KIND_R2C) {
+      V *X = reinterpret_cast<V *>(a.p.out) + oo;
+      if (a.odd) {
+        X[k * os] = A[gidx<COL>(tb, k, TB, L)];
+      } else {
+        V za = A[gidx<COL>(tb, k == L ? 0 : k, TB, L)];
+        V zb = cconj(A[gidx<COL>(tb, k == 0 ? 0 : L - k, TB, L)]);
+        V ev = cmake(T(0.5) * (za.x + zb.x), T(0.5) * (za.y + zb.y));
+        V d = csub(za, zb);
+        V ov = cmake(T(0.5) * d.y, T(-0.5) * d.x);
+        X[k * os] = cadd(ev, cmulw<false>(ov, ldtw(tw, k)));
+      }
+    } else { // C2R
+      T *x = reinterpret_cast<T *>(a.p.out) + oo;
+      V z = A[gidx<COL>(tb, k, TB, L)];
+      if (a.odd) {
+        x[k * os] = z.x;
+      } else {
+        x[(2LL * k) * os] = z.x;
+        x[(2LL * k + 1) * os] = z.y;
+      }
+    }
+  }
+}
+
+} // namespace b200fft

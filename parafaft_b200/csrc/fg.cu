@@ -1,0 +1,121 @@
+// Runtime-generic (Family G) kernels, the twiddle-table kernel and the
+// shared-memory size queries used by the planner.
+#include <climits>
+
+#include "fft_device.cuh"
+#include "launch.hpp"
+
+namespace b200fft {
+
+// ==========================================================================
+// Twiddle table exp(-2*pi*i*m/n), m in [0, n), computed in FP64.
+// 4m = q*n + r with integers q (quadrant) and r < n; the angle is
+// (pi/2)(q + r/n); the remainder is folded to [0, n/2] so sincospi gets an
+// argument in [0, 1/4] that carries no reduction error.
+// ==========================================================================
+__global__ void twiddle_table_kernel(double2 *t64, float2 *t32, int n) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n)
+    return;
+  const long long t = 4LL * m;
+  const int q = static_cast<int>(t / n);
+  const long long r = t - static_cast<long long>(q) * n;
+  const bool flip = 2 * r > n;
+  const long long rr = flip ? (n - r) : r;
+  double s, c;
+  sincospi(static_cast<double>(rr) / (2.0 * static_cast<double>(n)), &s, &c);
+  if (flip) {
+    const double tmp = s;
+    s = c;
+    c = tmp;
+  }
+  double cr, ci;
+  switch (q & 3) {
+  case 0: cr = c; ci = s; break;
+  case 1: cr = -s; ci = c; break;
+  case 2: cr = -c; ci = -s; break;
+  default: cr = s; ci = -c; break;
+  }
+  const double2 w = make_double2(cr, -ci);
+  if (t64)
+    t64[m] = w;
+  if (t32)
+    t32[m] = make_float2(static_cast<float>(w.x), static_cast<float>(w.y));
+}
+
+
+namespace {
+
+template <typename T> constexpr size_t smem_s(int L, bool col) {
+  const CfgS c = cfg_static(static_cast<int>(sizeof(cvec<T>)), L, col);
+  const int LP = col ? L : (L + L / 8);
+  return static_cast<size_t>(c.TB) * LP * sizeof(cvec<T>);
+}
+
+template <typename T, bool COL, int KIND, bool FWD>
+cudaError_t launch_g(const GenArgs &g, cudaStream_t st) {
+  auto kern = fft_generic_kernel<T, COL, KIND, FWD>;
+  const size_t smem = 2ull * g.TB * g.L * sizeof(cvec<T>);
+  if (smem > kGenericSmemLimit)
+    return cudaErrorInvalidValue;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kGenericSmemLimit));
+    if (e != cudaSuccess)
+      return e;
+  }
+  const long long grid = (g.p.total + g.TB - 1) / g.TB;
+  if (grid <= 0)
+    return cudaSuccess;
+  if (grid > INT_MAX)
+    return cudaErrorInvalidConfiguration;
+  kern<<<static_cast<unsigned>(grid), kGenThreads, smem, st>>>(g);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_g_t(int kind, bool col, bool fwd, const GenArgs &g,
+                       cudaStream_t st) {
+  if (kind == KIND_C2C) {
+    if (col)
+      return fwd ? launch_g<T, true, KIND_C2C, true>(g, st)
+                 : launch_g<T, true, KIND_C2C, false>(g, st);
+    return fwd ? launch_g<T, false, KIND_C2C, true>(g, st)
+               : launch_g<T, false, KIND_C2C, false>(g, st);
+  }
+  if (kind == KIND_R2C)
+    return col ? launch_g<T, true, KIND_R2C, true>(g, st)
+               : launch_g<T, false, KIND_R2C, true>(g, st);
+  return col ? launch_g<T, true, KIND_C2R, false>(g, st)
+             : launch_g<T, false, KIND_C2R, false>(g, st);
+}
+
+} // namespace
+
+cudaError_t launch_generic(bool f64, int kind, bool col, bool fwd,
+                           const GenArgs &g, cudaStream_t st) {
+  return f64 ? launch_g_t<double>(kind, col, fwd, g, st)
+             : launch_g_t<float>(kind, col, fwd, g, st);
+}
+
+size_t generic_smem_bytes(bool f64, int TB, int L) {
+  return 2ull * TB * L * (f64 ? sizeof(double2) : sizeof(float2));
+}
+
+size_t static_smem_bytes(int esize_complex, int L, bool col) {
+  if (!static_length_ok(L))
+    return 0;
+  return esize_complex == 16 ? smem_s<double>(L, col) : smem_s<float>(L, col);
+}
+
+cudaError_t launch_twiddle_table(double2 *t64, float2 *t32, int n,
+                                 cudaStream_t st) {
+  if (n <= 0)
+    return cudaErrorInvalidValue;
+  const int threads = 256;
+  const int blocks = (n + threads - 1) / threads;
+  twiddle_table_kernel<<<blocks, threads, 0, st>>>(t64, t32, n);
+  return cudaGetLastError();
+}
+
+} // namespace b200fft

@@ -1,0 +1,13 @@
+// Specialised C2C kernels, FP32 (column and row layouts, both directions).
+#include "fs_launch.cuh"
+
+namespace b200fft {
+cudaError_t launch_static_c2c_f32(int L, bool col, bool fwd, const PassArgs &a,
+                                  cudaStream_t st) {
+  if (col)
+    return fwd ? launch_static_switch<float, true, true, KIND_C2C>(L, a, st)
+               : launch_static_switch<float, true, false, KIND_C2C>(L, a, st);
+  return fwd ? launch_static_switch<float, false, true, KIND_C2C>(L, a, st)
+             : launch_static_switch<float, false, false, KIND_C2C>(L, a, st);
+}
+} // namespace b200fft

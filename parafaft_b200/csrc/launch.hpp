@@ -1,0 +1,36 @@
+// Host-side launchers of the transform kernels (defined in fs_*.cu / fg.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fft_common.hpp"
+
+namespace b200fft {
+
+// Family S: specialised kernels for power-of-two stage lengths L.
+// C2C: col selects the column thread mapping (strided points).
+cudaError_t launch_static_c2c_f32(int L, bool col, bool fwd, const PassArgs &a,
+                                  cudaStream_t st);
+cudaError_t launch_static_c2c_f64(int L, bool col, bool fwd, const PassArgs &a,
+                                  cudaStream_t st);
+// R2C (forward) / C2R (backward) of real length 2L, contiguous padded rows;
+// both sides of `a` in complex units.
+cudaError_t launch_static_r2c_f32(int L, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_static_c2r_f32(int L, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_static_r2c_f64(int L, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_static_c2r_f64(int L, const PassArgs &a, cudaStream_t st);
+
+// Shared-memory bytes of a Family S launch (0 when no kernel exists).
+size_t static_smem_bytes(int esize_complex, int L, bool col);
+
+// Family G: runtime-generic kernels.
+cudaError_t launch_generic(bool f64, int kind, bool col, bool fwd,
+                           const GenArgs &g, cudaStream_t st);
+size_t generic_smem_bytes(bool f64, int TB, int L);
+constexpr size_t kGenericSmemLimit = 200 * 1024;
+
+// FP64 twiddle table exp(-2*pi*i*m/n) (t64 and/or t32 may be null).
+cudaError_t launch_twiddle_table(double2 *t64, float2 *t32, int n,
+                                 cudaStream_t st);
+
+} // namespace b200fft

@@ -1,0 +1,189 @@
+// ParaFaFT's own orchestrators, ParaFaFT_C2C<D, Backend> and
+// ParaFaFT_R2C<D, Backend> (parafaft_c2c.hpp:69, parafaft_r2c.hpp:98),
+// instantiated with B200Backend<T> — the drop-in this project provides — and,
+// for comparison on the same GPU, with the reference CuFFTBackend<T>
+// (backend/cufft/fft_backend_cufft.hpp). A small C ABI exposes the objects to
+// the Python tests and the benchmark, so every transform they run goes through
+// the reference's forward()/backward() code path unchanged.
+//
+// Built only where the ParaFaFT headers are present. FFTW is not installed
+// here, so the FFTW backend header is skipped; ParaFaFT only names
+// FFTWBackend<> as a default template argument, which a declaration
+// satisfies.
+#define PARAFAFT_BACKEND_FFTW_HPP 1
+namespace parafaft {
+template <typename FloatTypeT = double> class FFTWBackend;
+}
+
+#include <mpi.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+
+#include "parafaft_c2c.hpp"
+#include "parafaft_r2c.hpp"
+
+#include "b200fft.h"
+#include "fft_backend_b200.hpp"
+
+namespace {
+
+thread_local std::string g_err;
+
+struct Obj {
+  virtual ~Obj() = default;
+  virtual void forward(void *data) = 0;
+  virtual void backward(void *data) = 0;
+  virtual void forward_oop(const void *in, void *out) = 0;
+  virtual void backward_oop(void *in, void *out) = 0;
+  virtual long long required_size() const = 0;
+  virtual void shapes(int *in_shape, int *in_start, int *out_shape, int *out_start) const = 0;
+  int ndim = 0;
+  bool r2c = false;
+  b200fft_handle handle = nullptr;
+};
+
+template <int D, class B> struct C2CObj : Obj {
+  using F = parafaft::ParaFaFT_C2C<D, B>;
+  using Cx = typename B::Complex;
+  std::unique_ptr<F> f;
+  C2CObj(const int *shape, parafaft::FFTPlanFlag flag) {
+    parafaft::b200_detail::last_opened() = nullptr;
+    f.reset(new F(shape, MPI_COMM_WORLD, flag));
+    handle = parafaft::b200_detail::last_opened();
+    this->ndim = D;
+  }
+  void forward(void *d) override { f->forward(static_cast<Cx *>(d)); }
+  void backward(void *d) override { f->backward(static_cast<Cx *>(d)); }
+  void forward_oop(const void *, void *) override {
+    throw std::runtime_error("out-of-place transforms exist for R2C objects only");
+  }
+  void backward_oop(void *, void *) override {
+    throw std::runtime_error("out-of-place transforms exist for R2C objects only");
+  }
+  long long required_size() const override {
+    return static_cast<long long>(f->get_required_output_size());
+  }
+  void shapes(int *a, int *b, int *c, int *d) const override {
+    f->get_local_shape(a);
+    f->get_global_start(b);
+    f->get_final_shape(c);
+    f->get_final_start(d);
+  }
+};
+
+template <int D, class B> struct R2CObj : Obj {
+  using F = parafaft::ParaFaFT_R2C<D, B>;
+  using Cx = typename B::Complex;
+  using Fl = typename B::FloatType;
+  std::unique_ptr<F> f;
+  R2CObj(const int *shape, parafaft::FFTPlanFlag flag) {
+    parafaft::b200_detail::last_opened() = nullptr;
+    f.reset(new F(shape, MPI_COMM_WORLD, flag));
+    handle = parafaft::b200_detail::last_opened();
+    this->ndim = D;
+    this->r2c = true;
+  }
+  void forward(void *d) override { f->forward_in_place(static_cast<Fl *>(d)); }
+  void backward(void *d) override { f->backward_in_place(static_cast<Fl *>(d)); }
+  void forward_oop(const void *in, void *out) override {
+    f->forward(static_cast<const Fl *>(in), static_cast<Cx *>(out));
+  }
+  void backward_oop(void *in, void *out) override {
+    f->backward(static_cast<Cx *>(in), static_cast<Fl *>(out));
+  }
+  long long required_size() const override {
+    return static_cast<long long>(f->get_required_output_size());
+  }
+  void shapes(int *a, int *b, int *c, int *d) const override {
+    f->get_local_real_shape(a);
+    f->get_real_global_start(b);
+    f->get_local_complex_shape(c);
+    f->get_complex_global_start(d);
+  }
+};
+
+template <template <int, class> class O, class B>
+Obj *make_d(int D, const int *shape, parafaft::FFTPlanFlag flag) {
+  switch (D) {
+  case 2: return new O<2, B>(shape, flag);
+  case 3: return new O<3, B>(shape, flag);
+  case 4: return new O<4, B>(shape, flag);
+  case 5: return new O<5, B>(shape, flag);
+  default: throw std::runtime_error("D must be 2..5");
+  }
+}
+
+template <template <int, class> class O>
+Obj *make(int D, int prec, int backend, const int *shape, int plan_flag) {
+  const auto flag = static_cast<parafaft::FFTPlanFlag>(plan_flag);
+  if (backend == 0)
+    return prec == B200FFT_F64 ? make_d<O, parafaft::B200Backend<double>>(D, shape, flag)
+                               : make_d<O, parafaft::B200Backend<float>>(D, shape, flag);
+  if (backend == 1)
+    return prec == B200FFT_F64 ? make_d<O, parafaft::CuFFTBackend<double>>(D, shape, flag)
+                               : make_d<O, parafaft::CuFFTBackend<float>>(D, shape, flag);
+  throw std::runtime_error("backend must be 0 (B200Backend) or 1 (CuFFTBackend)");
+}
+
+template <class F> int guard(F f) {
+  try {
+    f();
+    return 0;
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return -1;
+  } catch (...) {
+    g_err = "unknown exception";
+    return -1;
+  }
+}
+
+} // namespace
+
+extern "C" {
+
+const char *pfb_last_error(void) { return g_err.c_str(); }
+
+// kind: 0 C2C, 1 R2C. backend: 0 B200Backend, 1 CuFFTBackend. prec: B200FFT_F32/F64.
+int pfb_create(int kind, int D, int prec, int backend, const int *shape, int plan_flag,
+               void **out) {
+  return guard([&] {
+    *out = nullptr;
+    Obj *o = kind == 0 ? make<C2CObj>(D, prec, backend, shape, plan_flag)
+                       : make<R2CObj>(D, prec, backend, shape, plan_flag);
+    *out = o;
+  });
+}
+
+int pfb_destroy(void *h) {
+  return guard([&] { delete static_cast<Obj *>(h); });
+}
+
+int pfb_forward(void *h, void *data) {
+  return guard([&] { static_cast<Obj *>(h)->forward(data); });
+}
+
+int pfb_backward(void *h, void *data) {
+  return guard([&] { static_cast<Obj *>(h)->backward(data); });
+}
+
+int pfb_forward_oop(void *h, const void *in, void *out) {
+  return guard([&] { static_cast<Obj *>(h)->forward_oop(in, out); });
+}
+
+int pfb_backward_oop(void *h, void *in, void *out) {
+  return guard([&] { static_cast<Obj *>(h)->backward_oop(in, out); });
+}
+
+long long pfb_required_size(void *h) { return static_cast<Obj *>(h)->required_size(); }
+
+int pfb_shapes(void *h, int *in_shape, int *in_start, int *out_shape, int *out_start) {
+  return guard([&] { static_cast<Obj *>(h)->shapes(in_shape, in_start, out_shape, out_start); });
+}
+
+// The B200 handle inside the object (null for CuFFTBackend objects).
+void *pfb_b200_handle(void *h) { return static_cast<Obj *>(h)->handle; }
+
+} // extern "C"

@@ -1,0 +1,328 @@
+"""ctypes bindings of the two native libraries of parafaft_b200.
+
+* ``libb200fft.so`` — the transform engine's C ABI (include/b200fft.h).
+* ``libparafaft_b200_drivers.so`` — ParaFaFT_C2C / ParaFaFT_R2C objects (the
+  reference orchestrators, compiled against B200Backend or CuFFTBackend).
+
+Nothing here computes on the CPU: if a library is missing the loaders raise,
+and the engine itself refuses to create a handle without a CUDA device (except
+in record-only mode, which plans and counts launches but moves no data).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_DIR = Path(__file__).resolve().parent / "lib"
+ENGINE_PATH = LIB_DIR / "libb200fft.so"
+DRIVERS_PATH = LIB_DIR / "libparafaft_b200_drivers.so"
+
+F32, F64 = 0, 1
+FORWARD, BACKWARD = 0, 1
+PLAN_ESTIMATE, PLAN_MEASURE, PLAN_PATIENT = 0, 1, 2
+FLAG_NO_DEFER, FLAG_RECORD_ONLY, FLAG_GENERIC_ONLY = 1, 2, 4
+KIND_C2C, KIND_R2C, KIND_C2R = 0, 1, 2
+
+STATUS = {
+    0: "SUCCESS", -1: "INVALID_ARG", -2: "UNSUPPORTED", -3: "NO_PLAN", -4: "CUDA",
+    -5: "RANGE", -6: "NO_DEVICE", -7: "DEVICE_STATUS",
+}
+
+# Every symbol include/b200fft.h declares.
+ENGINE_SYMBOLS = (
+    "b200fft_last_error", "b200fft_version", "b200fft_device_count",
+    "b200fft_create", "b200fft_destroy", "b200fft_set_stream",
+    "b200fft_plan_c2c", "b200fft_exec_c2c", "b200fft_plan_r2c", "b200fft_exec_r2c",
+    "b200fft_plan_c2r", "b200fft_exec_c2r", "b200fft_memcpy", "b200fft_memcpy2d",
+    "b200fft_sync", "b200fft_flush", "b200fft_alloc", "b200fft_free",
+    "b200fft_get_stats", "b200fft_reset_stats", "b200fft_get_log", "b200fft_set_profiling",
+    "b200fft_describe", "b200fft_supported",
+)
+
+
+class B200FFTError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Stats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "kernel_launches", "exec_calls", "coalesced_calls", "memcpy_calls",
+        "fused_copies", "copies_issued", "bytes_copied", "bytes_transformed")]
+
+    def as_dict(self) -> dict:
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+class LaunchRecord(C.Structure):
+    _fields_ = [("kind", C.c_int), ("direction", C.c_int), ("stage", C.c_int),
+                ("family", C.c_int), ("length", C.c_int), ("fused_copy", C.c_int),
+                ("transforms", C.c_longlong), ("slabs", C.c_longlong),
+                ("bytes", C.c_longlong), ("ms", C.c_double)]
+
+    def as_dict(self) -> dict:
+        d = {n: int(getattr(self, n)) for n, _ in self._fields_ if n != "ms"}
+        d["ms"] = float(self.ms)
+        return d
+
+
+_engine = None
+_drivers = None
+
+
+def engine() -> C.CDLL:
+    """Load libb200fft.so (raises if it has not been built)."""
+    global _engine
+    if _engine is None:
+        if not ENGINE_PATH.exists():
+            raise ImportError(f"{ENGINE_PATH} is missing: run `python -m parafaft_b200.build`")
+        lib = C.CDLL(str(ENGINE_PATH))
+        vp, i, sz, pd = C.c_void_p, C.c_int, C.c_size_t, C.c_ssize_t
+        sig = {
+            "b200fft_last_error": (C.c_char_p, []),
+            "b200fft_version": (i, []),
+            "b200fft_device_count": (i, []),
+            "b200fft_create": (i, [i, i, i, C.c_uint, C.POINTER(vp)]),
+            "b200fft_destroy": (i, [vp]),
+            "b200fft_set_stream": (i, [vp, vp]),
+            "b200fft_plan_c2c": (i, [vp, i, i, sz, pd, pd]),
+            "b200fft_exec_c2c": (i, [vp, i, i, vp]),
+            "b200fft_plan_r2c": (i, [vp, i, sz, pd, pd]),
+            "b200fft_exec_r2c": (i, [vp, vp]),
+            "b200fft_plan_c2r": (i, [vp, i, sz, pd, pd]),
+            "b200fft_exec_c2r": (i, [vp, vp]),
+            "b200fft_memcpy": (i, [vp, vp, vp, sz]),
+            "b200fft_memcpy2d": (i, [vp, vp, sz, vp, sz, sz, sz]),
+            "b200fft_sync": (i, [vp]),
+            "b200fft_flush": (i, [vp]),
+            "b200fft_alloc": (i, [sz, C.POINTER(vp)]),
+            "b200fft_free": (i, [vp]),
+            "b200fft_get_stats": (i, [vp, C.POINTER(Stats)]),
+            "b200fft_reset_stats": (i, [vp]),
+            "b200fft_get_log": (i, [vp, C.POINTER(LaunchRecord), i, C.POINTER(i)]),
+            "b200fft_set_profiling": (i, [vp, i]),
+            "b200fft_describe": (i, [i, i, i, sz, pd, pd, C.c_char_p, sz]),
+            "b200fft_supported": (i, [i, i, i]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _engine = lib
+    return _engine
+
+
+def drivers() -> C.CDLL:
+    """Load the ParaFaFT driver library (raises if it has not been built)."""
+    global _drivers
+    if _drivers is None:
+        engine()  # resolve libb200fft first
+        if not DRIVERS_PATH.exists():
+            raise ImportError(f"{DRIVERS_PATH} is missing: build it where the ParaFaFT headers exist")
+        lib = C.CDLL(str(DRIVERS_PATH))
+        vp, i = C.c_void_p, C.c_int
+        ip = C.POINTER(C.c_int)
+        for name, res, args in (
+            ("pfb_last_error", C.c_char_p, []),
+            ("pfb_create", i, [i, i, i, i, ip, i, C.POINTER(vp)]),
+            ("pfb_destroy", i, [vp]),
+            ("pfb_forward", i, [vp, vp]),
+            ("pfb_backward", i, [vp, vp]),
+            ("pfb_forward_oop", i, [vp, vp, vp]),
+            ("pfb_backward_oop", i, [vp, vp, vp]),
+            ("pfb_required_size", C.c_longlong, [vp]),
+            ("pfb_shapes", i, [vp, ip, ip, ip, ip]),
+            ("pfb_b200_handle", vp, [vp]),
+        ):
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _drivers = lib
+    return _drivers
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise B200FFTError(rc, engine().b200fft_last_error().decode())
+
+
+def _ptr(x) -> int:
+    """Device/host address of a torch tensor, an int, or None."""
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    return int(x.data_ptr())
+
+
+class Handle:
+    """One engine handle (what a B200Backend<T> object owns)."""
+
+    def __init__(self, precision: int = F32, num_stages: int = 1,
+                 plan_flag: int = PLAN_ESTIMATE, flags: int = 0):
+        self._lib = engine()
+        h = C.c_void_p()
+        check(self._lib.b200fft_create(precision, num_stages, plan_flag, flags, C.byref(h)))
+        self._h = h
+        self.precision = precision
+
+    @classmethod
+    def wrap(cls, raw: int) -> "Handle":
+        """Borrow an existing handle (not destroyed by this object)."""
+        obj = cls.__new__(cls)
+        obj._lib = engine()
+        obj._h = C.c_void_p(raw)
+        obj.precision = None
+        obj._borrowed = True
+        return obj
+
+    @property
+    def raw(self) -> int:
+        return self._h.value or 0
+
+    def close(self) -> None:
+        if getattr(self, "_borrowed", False):
+            return
+        if self._h:
+            check(self._lib.b200fft_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def plan_c2c(self, stage, length, batch, stride, dist):
+        check(self._lib.b200fft_plan_c2c(self._h, stage, length, batch, stride, dist))
+
+    def exec_c2c(self, stage, direction, data):
+        check(self._lib.b200fft_exec_c2c(self._h, stage, direction, _ptr(data)))
+
+    def plan_r2c(self, length, batch, stride, dist):
+        check(self._lib.b200fft_plan_r2c(self._h, length, batch, stride, dist))
+
+    def exec_r2c(self, data):
+        check(self._lib.b200fft_exec_r2c(self._h, _ptr(data)))
+
+    def plan_c2r(self, length, batch, stride, dist):
+        check(self._lib.b200fft_plan_c2r(self._h, length, batch, stride, dist))
+
+    def exec_c2r(self, data):
+        check(self._lib.b200fft_exec_c2r(self._h, _ptr(data)))
+
+    def memcpy(self, dst, src, nbytes):
+        check(self._lib.b200fft_memcpy(self._h, _ptr(dst), _ptr(src), nbytes))
+
+    def memcpy2d(self, dst, dpitch, src, spitch, width, height):
+        check(self._lib.b200fft_memcpy2d(self._h, _ptr(dst), dpitch, _ptr(src), spitch,
+                                         width, height))
+
+    def set_stream(self, stream: int | None):
+        check(self._lib.b200fft_set_stream(self._h, stream or 0))
+
+    def sync(self):
+        check(self._lib.b200fft_sync(self._h))
+
+    def flush(self):
+        check(self._lib.b200fft_flush(self._h))
+
+    def stats(self) -> dict:
+        s = Stats()
+        check(self._lib.b200fft_get_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def reset_stats(self):
+        check(self._lib.b200fft_reset_stats(self._h))
+
+    def set_profiling(self, on: bool = True):
+        check(self._lib.b200fft_set_profiling(self._h, 1 if on else 0))
+
+    def log(self, cap: int = 4096) -> list[dict]:
+        buf = (LaunchRecord * cap)()
+        n = C.c_int()
+        check(self._lib.b200fft_get_log(self._h, buf, cap, C.byref(n)))
+        return [buf[i].as_dict() for i in range(n.value)]
+
+
+def describe(precision: int, kind: int, length: int, batch: int = 1, stride: int = 1,
+             dist: int | None = None) -> str:
+    if dist is None:
+        dist = length if kind == KIND_C2C else 2 * (length // 2 + 1)
+    buf = C.create_string_buffer(256)
+    check(engine().b200fft_describe(precision, kind, length, batch, stride, dist, buf, 256))
+    return buf.value.decode()
+
+
+def supported(precision: int, kind: int, length: int) -> bool:
+    return bool(engine().b200fft_supported(precision, kind, length))
+
+
+class ParaFaFT:
+    """A ParaFaFT_C2C<D, B> or ParaFaFT_R2C<D, B> object of the reference code.
+
+    kind: "c2c" or "r2c"; backend: "b200" (B200Backend<T>) or "cufft"
+    (the reference CuFFTBackend<T>, for comparison). Data arguments are device
+    pointers (ints) or CUDA torch tensors.
+    """
+
+    def __init__(self, kind: str, shape, precision: int = F32, backend: str = "b200",
+                 plan_flag: int = PLAN_ESTIMATE):
+        self._lib = drivers()
+        self.kind = kind
+        self.shape = tuple(int(s) for s in shape)
+        self.D = len(self.shape)
+        self.precision = precision
+        arr = (C.c_int * self.D)(*self.shape)
+        h = C.c_void_p()
+        rc = self._lib.pfb_create(0 if kind == "c2c" else 1, self.D, precision,
+                                  0 if backend == "b200" else 1, arr, plan_flag, C.byref(h))
+        if rc != 0:
+            raise RuntimeError("ParaFaFT construction failed: " + self._lib.pfb_last_error().decode())
+        self._h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(self._lib.pfb_last_error().decode())
+
+    def close(self):
+        if self._h:
+            self._check(self._lib.pfb_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, data):
+        """C2C forward() / R2C forward_in_place()."""
+        self._check(self._lib.pfb_forward(self._h, _ptr(data)))
+
+    def backward(self, data):
+        """C2C backward() / R2C backward_in_place()."""
+        self._check(self._lib.pfb_backward(self._h, _ptr(data)))
+
+    def forward_oop(self, real_in, complex_out):
+        self._check(self._lib.pfb_forward_oop(self._h, _ptr(real_in), _ptr(complex_out)))
+
+    def backward_oop(self, complex_in, real_out):
+        self._check(self._lib.pfb_backward_oop(self._h, _ptr(complex_in), _ptr(real_out)))
+
+    @property
+    def required_size(self) -> int:
+        """get_required_output_size(): Complex elements (C2C) / FloatType scalars (R2C)."""
+        return int(self._lib.pfb_required_size(self._h))
+
+    def shapes(self) -> dict:
+        a, b, c, d = ((C.c_int * self.D)() for _ in range(4))
+        self._check(self._lib.pfb_shapes(self._h, a, b, c, d))
+        return {"in_shape": list(a), "in_start": list(b), "out_shape": list(c),
+                "out_start": list(d)}
+
+    def handle(self) -> Handle | None:
+        raw = self._lib.pfb_b200_handle(self._h)
+        return Handle.wrap(raw) if raw else None

@@ -1,0 +1,154 @@
+"""Host-side logic on the CPU: the C ABI's exports, kernel selection, and the
+deferral/fusion bookkeeping of the backend, run with the real ParaFaFT
+orchestrators in record-only mode (plans and counts, no GPU work)."""
+import ctypes as C
+import os
+import re
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+from parafaft_b200 import native as nv
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _declared_symbols():
+    text = (ROOT / "include" / "b200fft.h").read_text()
+    return sorted(set(re.findall(r"\b(b200fft_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = nv.engine()
+    declared = _declared_symbols()
+    assert declared, "no declarations found"
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+    assert sorted(nv.ENGINE_SYMBOLS) == declared
+
+
+def test_version_and_no_device_refusal():
+    lib = nv.engine()
+    assert lib.b200fft_version() >= 100
+    if lib.b200fft_device_count() == 0:
+        with pytest.raises(nv.B200FFTError) as e:
+            nv.Handle(nv.F32, 1)
+        assert e.value.code == -6  # NO_DEVICE: no CPU fallback
+
+
+def test_argument_validation():
+    h = nv.Handle(nv.F32, 2, flags=nv.FLAG_RECORD_ONLY)
+    with pytest.raises(nv.B200FFTError):
+        h.plan_c2c(5, 64, 1, 1, 64)          # stage out of range
+    with pytest.raises(nv.B200FFTError):
+        h.plan_c2c(0, 0, 1, 1, 64)           # zero length
+    with pytest.raises(nv.B200FFTError) as e:
+        h.exec_c2c(1, nv.FORWARD, 4096)      # no plan
+    assert e.value.code == -3
+    with pytest.raises(nv.B200FFTError) as e:
+        h.plan_c2c(0, 67 * 71, 1, 1, 67 * 71)  # prime factors above 61
+    assert e.value.code == -2
+    with pytest.raises(nv.B200FFTError):
+        h.exec_r2c(4096)                     # no r2c plan
+
+
+@pytest.mark.parametrize("kind,n,expect", [
+    (nv.KIND_C2C, 512, "static c2c L=512"), (nv.KIND_C2C, 60, "generic c2c L=60"),
+    (nv.KIND_R2C, 512, "static r2c L=256"), (nv.KIND_R2C, 63, "generic r2c L=63"),
+    (nv.KIND_C2R, 160, "generic c2r L=80"), (nv.KIND_C2C, 4096, "static c2c L=4096"),
+])
+def test_kernel_selection(kind, n, expect):
+    assert nv.describe(nv.F32, kind, n).startswith(expect)
+
+
+def test_supported_lengths():
+    assert nv.supported(nv.F32, nv.KIND_C2C, 4096)
+    assert nv.supported(nv.F64, nv.KIND_R2C, 3 * 7 * 61)
+    assert not nv.supported(nv.F64, nv.KIND_R2C, 3 * 5 * 7 * 61)  # above the one-pass limit
+    assert not nv.supported(nv.F32, nv.KIND_C2C, 127)  # prime above 61
+
+
+def test_fastdiv_restatement():
+    """The multiply-shift division used by the generic kernel (fft_common.hpp),
+    restated here and checked exhaustively on the divisors the planner uses."""
+    def make(d):
+        if d <= 1:
+            return 0, 0
+        l = (d - 1).bit_length()
+        return ((1 << (31 + l)) + d - 1) // d, l - 1
+    import random
+    rnd = random.Random(0)
+    for d in list(range(1, 300)) + [4095, 4096, 4097, 65536, 2**31 - 1]:
+        m, s = make(d)
+        assert m < 2**32
+        for n in [0, 1, d - 1, d, d + 1, 2**31 - 1] + [rnd.randrange(2**31) for _ in range(200)]:
+            q = n if m == 0 else ((n * m) >> 32) >> s
+            assert q == n // d, (n, d)
+
+
+def _run_record(script: str) -> str:
+    env = dict(os.environ, B200FFT_RECORD_ONLY="1")
+    r = subprocess.run([sys.executable, "-c", script], env=env, capture_output=True,
+                       text=True, cwd=ROOT, timeout=300)
+    assert r.returncode == 0, r.stderr
+    return r.stdout
+
+
+def _drivers_built():
+    return nv.DRIVERS_PATH.exists()
+
+
+@pytest.mark.skipif(not _drivers_built(), reason="ParaFaFT drivers not built")
+def test_r2c_512_cube_call_sequence_fuses_to_six_launches():
+    """ParaFaFT_R2C<3, B200Backend<float>> at 512^3: 2 x (1 + 512 + 1) backend
+    calls plus 4 exchange copies become 6 launches moving the algorithmic
+    6 463 422 464 bytes, with no copy issued."""
+    out = _run_record(r'''
+import ctypes as C
+from parafaft_b200 import native as nv
+f = nv.ParaFaFT("r2c", (512, 512, 512), nv.F32)
+buf = C.c_void_p(); nv.check(nv.engine().b200fft_alloc(f.required_size * 4, C.byref(buf)))
+f.forward(buf.value); f.backward(buf.value)
+st = f.handle().stats(); log = f.handle().log()
+print(st["kernel_launches"], st["exec_calls"], st["coalesced_calls"], st["fused_copies"],
+      st["copies_issued"], st["bytes_transformed"])
+print([(r["kind"], r["stage"], r["slabs"], r["fused_copy"]) for r in log])
+''')
+    first, second = out.strip().splitlines()
+    assert first.split() == ["6", "1028", "1022", "4", "0", "6463422464"]
+    assert second == ("[(1, -1, 1, 0), (0, 1, 512, 1), (0, 2, 1, 1), (0, 2, 1, 0), "
+                      "(0, 1, 512, 1), (2, -1, 1, 1)]")
+
+
+@pytest.mark.skipif(not _drivers_built(), reason="ParaFaFT drivers not built")
+@pytest.mark.parametrize("shape,launches", [((64, 64, 64), 6), ((1024, 1024, 1024), 6),
+                                           ((16, 16, 16, 16), 8), ((32, 32), 4)])
+def test_c2c_call_sequences(shape, launches):
+    out = _run_record(rf'''
+import ctypes as C
+from parafaft_b200 import native as nv
+f = nv.ParaFaFT("c2c", {shape!r}, nv.F64)
+buf = C.c_void_p(); nv.check(nv.engine().b200fft_alloc(f.required_size * 16, C.byref(buf)))
+f.forward(buf.value); f.backward(buf.value)
+st = f.handle().stats()
+print(st["kernel_launches"], st["copies_issued"], st["fused_copies"], st["memcpy_calls"])
+''')
+    k, copies, fused, calls = map(int, out.split())
+    assert k == launches and copies == 0 and fused == calls
+
+
+@pytest.mark.skipif(not _drivers_built(), reason="ParaFaFT drivers not built")
+def test_no_defer_issues_every_call():
+    out = _run_record(r'''
+import os, ctypes as C
+os.environ["B200FFT_NO_DEFER"] = "1"
+from parafaft_b200 import native as nv
+f = nv.ParaFaFT("r2c", (32, 32, 32), nv.F32)
+buf = C.c_void_p(); nv.check(nv.engine().b200fft_alloc(f.required_size * 4, C.byref(buf)))
+f.forward(buf.value)
+st = f.handle().stats()
+print(st["kernel_launches"], st["copies_issued"])
+''')
+    assert out.split() == ["34", "2"]
