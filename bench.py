@@ -42,6 +42,12 @@ METRIC = "512^3 FP32 R2C fwd+bwd ms, % HBM roofline; plain vs split-TC at rel-L2
 WORKLOAD = "ParaFaFT_R2C<3, float> 512x512x512 forward_in_place+backward_in_place"
 ALG_BYTES = 6463422464  # one read + one write per fused pass, fwd+bwd
 
+# DRAM bytes (read + write) per launch from the last `ncu --set full` capture
+# of the same kernels (profiles/r2c512_kernels_ncu_full.md).
+NCU_TRAFFIC = {"r2c_fwd": 1020480000, "c2c_stage1_fwd": 1030265344,
+               "c2c_stage2_fwd": 1029780480, "c2c_stage2_bwd": 1018808576,
+               "c2c_stage1_bwd": 1031222528, "c2r_bwd": 1041284864}
+
 
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
@@ -52,57 +58,82 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled through NVML every few
+    milliseconds while the timed region runs (nvidia-smi's 100 ms minimum
+    period is longer than short timed regions)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[tuple[int, int]] = []
+        self._stop = threading.Event()
+        self._t = None
+        self.err = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
-            self._t.start()
-        except FileNotFoundError:
-            self.proc = None
+            import pynvml as N
+            N.nvmlInit()
+            import torch
+            p = torch.cuda.get_device_properties(self.gpu)
+            h = None
+            if hasattr(p, "pci_bus_id"):
+                bus = "%08x:%02x:%02x.0" % (getattr(p, "pci_domain_id", 0), p.pci_bus_id,
+                                            getattr(p, "pci_device_id", 0))
+                try:
+                    h = N.nvmlDeviceGetHandleByPciBusId(bus)
+                except Exception:
+                    h = None
+            if h is None:
+                vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+                idx = int(vis.split(",")[self.gpu]) if vis and vis.split(",")[0].isdigit() else self.gpu
+                h = N.nvmlDeviceGetHandleByIndex(idx)
+            self._N, self._h = N, h
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+        except Exception as e:  # clocks are reported as unavailable
+            self.err = str(e)
+            return
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        N, h = self._N, self._h
+        while not self._stop.is_set():
+            try:
+                t = time.perf_counter()
+                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                rs = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((t, sm, rs))
+            except Exception as e:
+                self.err = str(e)
+                return
+            time.sleep(0.002)
+
+    def mark(self, which: str):
+        setattr(self, which, time.perf_counter())
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
+        """Samples taken between mark('t0') and mark('t1') (the timed region);
+        when the region is shorter than one NVML round trip, the samples
+        nearest to it on either side."""
+        if self._t is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "note": f"clock sampling unavailable: {self.err}"}
+        self._stop.set()
+        self._t.join(timeout=2)
+        t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", float("inf"))
+        inside = [x for x in self.samples if t0 <= x[0] <= t1]
+        if not inside and self.samples:
+            before = [x for x in self.samples if x[0] < t0][-1:]
+            after = [x for x in self.samples if x[0] > t1][:1]
+            inside = before + after
+        sm = [x[1] for x in inside]
+        reasons = sorted({n for x in inside for n, bit in self.REASONS.items() if x[2] & bit})
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "sm_max_mhz": self.max_mhz, "reasons": reasons, "samples": len(sm)}
 
 
 def make_input():
@@ -165,6 +196,24 @@ def run_reference(args):
     return 0
 
 
+def run_kernels_only(args):
+    """The timed loop alone (no checks, no comparators): the command profiled
+    under ncu."""
+    import torch
+    from parafaft_b200 import native as nv
+    torch.cuda.set_device(0)
+    host_buf, _ = make_input()
+    fft = nv.ParaFaFT("r2c", SHAPE, nv.F32)
+    dev = torch.from_numpy(host_buf).cuda()
+    for _ in range(args.warmup + args.steps):
+        fft.forward(dev)
+        fft.backward(dev)
+    torch.cuda.synchronize()
+    print("kernels-only done", fft.handle().stats()["kernel_launches"])
+    fft.close()
+    return 0
+
+
 def run_b200(args):
     import torch
     from parafaft_b200 import native as nv
@@ -222,11 +271,13 @@ def run_b200(args):
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    clocks.mark("t0")
     e0.record(stream)
     for _ in range(args.steps):
         step()
     e1.record(stream)
     torch.cuda.synchronize()
+    clocks.mark("t1")
     if pg:
         pg.barrier()
     clk = clocks.stop()
@@ -324,7 +375,8 @@ def run_b200(args):
             "hbm_roofline_frac_step": round(ALG_BYTES / (ms * 1e-3) / 1e9 / peak, 4),
             "gflops_5nlogn": round(2 * 5 * np.prod(SHAPE) * 27 / (ms * 1e-3) / 1e9, 1),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": peak,
-                         "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+                         "unit": "GB/s", "frac": round(ach / peak, 4),
+                         "traffic": NCU_TRAFFIC.get(dom), "traffic_source": "ncu capture",
                          "peak_source": peak_kind},
             "kernels": kernels,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": nbytes,
@@ -352,11 +404,15 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=150.0)
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="run only the timed loop (used for ncu captures)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernels_only:
+        return run_kernels_only(args)
     return run_b200(args)
 
 

@@ -68,6 +68,7 @@ struct Choice {
   int L = 0;      // complex points of the stage loop
   int tlen = 0;   // twiddle table length
   int TB = 0, NT = 0;
+  int variant = 0; // tile-shape candidate of a specialised kernel
   GenArgs gen{};
 };
 
@@ -131,6 +132,17 @@ int ilog2(int x) {
   return l;
 }
 
+// Tile-shape candidate used without autotuning. Column passes whose points
+// lie 4 MiB or more apart (the first axis of large grids) read wider
+// contiguous segments per point row with the wide tile; everything else uses
+// the full tile (measured on the 512^3 and 1024^3 passes).
+int default_variant(int csize, int L, bool col, long long stride) {
+  (void)L;
+  if (col && stride * csize >= (4ll << 20))
+    return 3;
+  return 0;
+}
+
 // Choose the kernel for a plan. kind: KIND_C2C/R2C/C2R.
 int choose_kernel(int prec, int kind, int len, long long batch, long long stride,
                   long long dist, bool force_generic, Choice *out) {
@@ -152,7 +164,12 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
       !force_generic && static_length_ok(L) &&
       (kind == KIND_C2C || (!odd && stride == 1 && dist % 2 == 0 && L <= 2048));
   if (static_ok) {
-    const CfgS c = cfg_static(csize, L, ch.col);
+    int var = default_variant(csize, L, ch.col, stride);
+    if (const char *v = std::getenv("B200FFT_VARIANT"))
+      if (v[0] >= '0' && v[0] < '0' + kStaticVariants && v[1] == '\0')
+        var = v[0] - '0';
+    const CfgS c = cfg_static(csize, L, ch.col, var);
+    ch.variant = var;
     ch.family = 0;
     ch.TB = c.TB;
     ch.NT = c.NT;
@@ -222,9 +239,9 @@ std::string describe_choice(const Choice &ch, int kind) {
   if (rad.empty())
     rad = "1";
   const char *kn = kind == KIND_C2C ? "c2c" : (kind == KIND_R2C ? "r2c" : "c2r");
-  std::snprintf(buf, sizeof(buf), "%s %s L=%d %s tb=%d nt=%d radices=%s",
+  std::snprintf(buf, sizeof(buf), "%s %s L=%d %s tb=%d nt=%d radices=%s var=%d",
                 ch.family == 0 ? "static" : "generic", kn, ch.L,
-                ch.col ? "col" : "row", ch.TB, ch.NT, rad.c_str());
+                ch.col ? "col" : "row", ch.TB, ch.NT, rad.c_str(), ch.variant);
   return buf;
 }
 
@@ -513,14 +530,14 @@ int launch_pass(H *h, const Plan &p, int dir, const void *in, void *out,
   cudaError_t e;
   if (p.ch.family == 0) {
     if (p.kind == KIND_C2C)
-      e = f64 ? launch_static_c2c_f64(p.ch.L, p.ch.col, fwd, a, h->stream)
-              : launch_static_c2c_f32(p.ch.L, p.ch.col, fwd, a, h->stream);
+      e = f64 ? launch_static_c2c_f64(p.ch.L, p.ch.col, fwd, p.ch.variant, a, h->stream)
+              : launch_static_c2c_f32(p.ch.L, p.ch.col, fwd, p.ch.variant, a, h->stream);
     else if (p.kind == KIND_R2C)
-      e = f64 ? launch_static_r2c_f64(p.ch.L, a, h->stream)
-              : launch_static_r2c_f32(p.ch.L, a, h->stream);
+      e = f64 ? launch_static_r2c_f64(p.ch.L, p.ch.variant, a, h->stream)
+              : launch_static_r2c_f32(p.ch.L, p.ch.variant, a, h->stream);
     else
-      e = f64 ? launch_static_c2r_f64(p.ch.L, a, h->stream)
-              : launch_static_c2r_f32(p.ch.L, a, h->stream);
+      e = f64 ? launch_static_c2r_f64(p.ch.L, p.ch.variant, a, h->stream)
+              : launch_static_c2r_f32(p.ch.L, p.ch.variant, a, h->stream);
   } else {
     GenArgs g = p.ch.gen;
     g.p = a;

@@ -137,9 +137,23 @@ struct CfgS {
 constexpr int ce_min(int a, int b) { return a < b ? a : b; }
 constexpr int ce_max(int a, int b) { return a > b ? a : b; }
 
-constexpr CfgS cfg_static(int esize, int L, bool col) {
-  const int NT = 256;
-  const int target = esize == 8 ? 8192 : 4096; // esize = sizeof(complex)
+// `variant` selects the tile shape among the candidates the planner (and its
+// autotuner) choose from:
+//   column layout: 0 = full tile, 1 = half, 2 = quarter (more CTAs per SM,
+//                  fewer registers per thread);
+//   row layout:    0 = default points per thread, 1 = twice, 2 = half.
+//   3 = wide column tile: 512 threads and twice the full tile, so every
+//       point row is read as one longer contiguous segment;
+//   4 = staged column pass: persistent CTAs of 512 threads, full tile,
+//       cp.async double buffering (one CTA per SM).
+constexpr int kStaticVariants = 5;
+constexpr int kVariantStaged = 4;
+
+constexpr CfgS cfg_static(int esize, int L, bool col, int variant = 0) {
+  const int NT = (col && (variant == 3 || variant == 4)) ? 512 : 256;
+  const int base = esize == 8 ? 8192 : 4096;
+  const int target =
+      col ? (variant == 3 ? 2 * base : (variant == 4 ? base : (base >> variant))) : base;
   const int emax = esize == 8 ? 32 : 16;
   if (col) {
     int TB = ce_min(NT, ce_max(1, target / L));
@@ -152,9 +166,17 @@ constexpr CfgS cfg_static(int esize, int L, bool col) {
   int E = L / 32;
   if (E < 8)
     E = ce_min(8, L);
+  if (variant == 1)
+    E *= 2;
+  else if (variant == 2 && E > 8)
+    E /= 2;
   if (E > emax)
     E = emax;
+  if (E > L)
+    E = L;
   int P = L / E;
+  if (P > NT)
+    P = NT;
   int TB = NT / P;
   return CfgS{NT, TB, P, E};
 }

@@ -141,16 +141,66 @@ template <int R, bool FWD, typename V> BF_D void dft(V *v) {
 
 template <typename V> BF_D V ldtw(const V *tw, int m) { return __ldg(tw + m); }
 
+// Asynchronous global->shared copies (cp.async): the data goes to shared
+// memory without passing through registers; a commit group per tile lets a CTA
+// wait for one tile while the next is still in flight.
+template <typename V> BF_D void cp_async_elem(V *smem, const V *gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  if constexpr (sizeof(V) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+BF_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> BF_D void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// v[r] *= w^r (r = 1..R-1), w^r = tw[r*base] (conjugated when CONJ). Radix 4
+// and 8 load w, w^2 (and w^4) and form the other powers by one complex
+// product each, which cuts table traffic from R-1 loads to 2 or 3.
+template <int R, bool CONJ, typename V>
+BF_D void apply_twiddles(V *v, const V *tw, int base) {
+  if constexpr (R == 2) {
+    v[1] = cmulw<CONJ>(v[1], ldtw(tw, base));
+  } else if constexpr (R == 4) {
+    const V w1 = ldtw(tw, base), w2 = ldtw(tw, 2 * base);
+    const V w3 = cmulw<false>(w1, w2);
+    v[1] = cmulw<CONJ>(v[1], w1);
+    v[2] = cmulw<CONJ>(v[2], w2);
+    v[3] = cmulw<CONJ>(v[3], w3);
+  } else if constexpr (R == 8) {
+    const V w1 = ldtw(tw, base), w2 = ldtw(tw, 2 * base), w4 = ldtw(tw, 4 * base);
+    const V w3 = cmulw<false>(w1, w2);
+    v[1] = cmulw<CONJ>(v[1], w1);
+    v[2] = cmulw<CONJ>(v[2], w2);
+    v[3] = cmulw<CONJ>(v[3], w3);
+    v[4] = cmulw<CONJ>(v[4], w4);
+    v[5] = cmulw<CONJ>(v[5], cmulw<false>(w4, w1));
+    v[6] = cmulw<CONJ>(v[6], cmulw<false>(w4, w2));
+    v[7] = cmulw<CONJ>(v[7], cmulw<false>(w4, w3));
+  } else {
+#pragma unroll
+    for (int r = 1; r < R; ++r)
+      v[r] = cmulw<CONJ>(v[r], ldtw(tw, r * base));
+  }
+}
+
 // ==========================================================================
 // Family S: lengths known at compile time (powers of two up to 4096).
 // ==========================================================================
-template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND>
+template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND,
+          bool STAGED = false>
 struct KS {
   using V = cvec<T>;
   static constexpr SchedS<L> S{};
   static constexpr int NST = S.nst;
   static constexpr int P = NT / TB; // threads per transform
-  static constexpr int LP = COL ? L : (L + L / 8);
+  // Row layouts pad one element every 16 (8-byte elements) or 8 (16-byte
+  // elements) so that both contiguous reads and the stride-R writes of the
+  // Stockham stages hit every bank equally.
+  static constexpr int PADSH = sizeof(V) == 8 ? 4 : 3;
+  static constexpr int LP = COL ? L : (L + (L >> PADSH));
   static constexpr int TSCALE = (KIND == KIND_C2C) ? 1 : 2;
   static constexpr bool WARP_SYNC = !COL && (P <= 32) && (32 % P == 0);
   static_assert(NT % TB == 0, "TB must divide NT");
@@ -169,7 +219,7 @@ struct KS {
   static constexpr int EMAX = emax();
 
   static constexpr size_t smem_bytes() {
-    return static_cast<size_t>(TB) * LP * sizeof(V);
+    return static_cast<size_t>(TB) * LP * sizeof(V) * (STAGED ? 2 : 1);
   }
 
   struct Ctx {
@@ -192,11 +242,12 @@ struct KS {
     if constexpr (COL)
       return n * TB + c.tb;
     else
-      return c.tb * LP + n + (n >> 3);
+      return c.tb * LP + n + (n >> PADSH);
   }
 
   // C2R input: Z[n] = E + i*O from X[n] and X[L-n] (real length 2L).
-  static BF_D V c2r_pre(const Ctx &c, int n) {
+  // w = exp(-2*pi*i*n/(2L)).
+  static BF_D V c2r_pre(const Ctx &c, int n, V w) {
     V xa = c.gin[(long long)n * c.ist];
     V xb = c.gin[(long long)(L - n) * c.ist];
     if (n == 0) {
@@ -204,18 +255,19 @@ struct KS {
       xb.y = T(0);
     }
     V e = cadd(xa, cconj(xb));
-    V o = cmulw<true>(csub(xa, cconj(xb)), ldtw(c.tw, n));
+    V o = cmulw<true>(csub(xa, cconj(xb)), w);
     return cmake(e.x - o.y, e.y + o.x);
   }
 
   // R2C output k in [0, L] from Z held in shared memory (natural order).
-  static BF_D V r2c_post(const Ctx &c, int k) {
+  // w = exp(-2*pi*i*k/(2L)).
+  static BF_D V r2c_post(const Ctx &c, int k, V w) {
     V a = c.sm[sidx(c, k == L ? 0 : k)];
     V b = cconj(c.sm[sidx(c, k == 0 ? 0 : L - k)]);
     V e = cmake(T(0.5) * (a.x + b.x), T(0.5) * (a.y + b.y));
     V d = csub(a, b);
     V o = cmake(T(0.5) * d.y, T(-0.5) * d.x); // -i*(a-b)/2
-    return cadd(e, cmulw<false>(o, ldtw(c.tw, k)));
+    return cadd(e, cmulw<false>(o, w));
   }
 
   template <int s> static BF_D void run(Ctx &c, V (&v)[EMAX]) {
@@ -230,11 +282,7 @@ struct KS {
         const int j = c.g + P * i;
         if (FULL || j < B) {
           const int k = j % Ns;
-#pragma unroll
-          for (int r = 1; r < R; ++r) {
-            const int e = r * k * (L / (Ns * R));
-            v[i * R + r] = cmulw<!FWD>(v[i * R + r], ldtw(c.tw, e * TSCALE));
-          }
+          apply_twiddles<R, !FWD>(&v[i * R], c.tw, k * (L / (Ns * R)) * TSCALE);
         }
       }
     }
@@ -256,12 +304,16 @@ struct KS {
           }
         }
         bar();
+        // exp(-2*pi*i*(g + P*i)/(2L)) = tw[g] * tw[P*i]; tw[P*i] is the
+        // same for every thread (a broadcast load).
         constexpr int KO = (L + 1 + P - 1) / P;
+        const V wg = ldtw(c.tw, c.g);
 #pragma unroll
         for (int i = 0; i < KO; ++i) {
           const int k = c.g + P * i;
           if (c.act && k <= L)
-            c.gout[(long long)k * c.ost] = r2c_post(c, k);
+            c.gout[(long long)k * c.ost] =
+                r2c_post(c, k, i == 0 ? wg : cmulw<false>(wg, ldtw(c.tw, P * i)));
         }
       } else {
         if (c.act) {
@@ -277,7 +329,7 @@ struct KS {
         }
       }
     } else {
-      if constexpr (s > 0)
+      if constexpr (s > 0 || STAGED)
         bar();
 #pragma unroll
       for (int i = 0; i < K; ++i) {
@@ -337,16 +389,98 @@ struct KS {
     for (int i = 0; i < K; ++i) {
       const int j = c.g + P * i;
       const bool ok = c.act && (FULL || j < B);
+      V wj;
+      if constexpr (KIND == KIND_C2R)
+        wj = ldtw(c.tw, j < B ? j : 0);
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int n = j + r * B;
-        if constexpr (KIND == KIND_C2R)
-          v[i * R + r] = ok ? c2r_pre(c, n) : czero<V>();
+        if constexpr (KIND == KIND_C2R) // tw[j + r*B] = tw[j] * tw[r*B]
+          v[i * R + r] =
+              ok ? c2r_pre(c, n, r == 0 ? wj : cmulw<false>(wj, ldtw(c.tw, r * B)))
+                 : czero<V>();
         else
           v[i * R + r] = ok ? c.gin[(long long)n * c.ist] : czero<V>();
       }
     }
     run<0>(c, v);
+  }
+
+  // ---- persistent column pass with cp.async double buffering -------------
+  // CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ...; while tile t is
+  // transformed in one shared buffer, the points of the next tile stream into
+  // the other, so loads stay in flight through the compute phases. Each tile
+  // holds TB adjacent transforms, L points each, as [point][transform].
+  static BF_D void prefetch(const PassArgs &a, V *buf, long long tile) {
+    static_assert(NT % TB == 0, "whole rows per pass");
+    const int tb = threadIdx.x % TB;
+    const int n0 = threadIdx.x / TB;
+    const long long b = tile * TB + tb;
+    if (b >= a.total)
+      return;
+    const long long sl = b / a.batch;
+    const long long w = b - sl * a.batch;
+    const V *g = reinterpret_cast<const V *>(a.in) + sl * a.islab + w * a.idist;
+    constexpr int ROWS = NT / TB;
+#pragma unroll 8
+    for (int n = n0; n < L; n += ROWS)
+      cp_async_elem(buf + n * TB + tb, g + static_cast<long long>(n) * a.istride);
+  }
+
+  static BF_D void entry_staged(const PassArgs &a, V *smem) {
+    static_assert(COL && KIND == KIND_C2C && STAGED, "staged path is for column C2C");
+    const long long ntiles = (a.total + TB - 1) / TB;
+    long long tile = blockIdx.x;
+    if (tile >= ntiles)
+      return;
+    V *const buf0 = smem;
+    V *const buf1 = smem + static_cast<size_t>(L) * TB;
+    prefetch(a, buf0, tile);
+    cp_async_commit();
+    Ctx c;
+    const int tid = threadIdx.x;
+    c.g = tid / TB;
+    c.tb = tid % TB;
+    c.tw = reinterpret_cast<const V *>(a.tw);
+    c.ist = a.istride;
+    c.ost = a.ostride;
+    c.gin = nullptr;
+    for (int it = 0;; ++it) {
+      const long long next = tile + gridDim.x;
+      if (next < ntiles)
+        prefetch(a, (it & 1) ? buf0 : buf1, next);
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();
+      c.sm = (it & 1) ? buf1 : buf0;
+      const long long b = tile * TB + c.tb;
+      c.act = b < a.total;
+      long long ooff = 0;
+      if (c.act) {
+        const long long sl = b / a.batch;
+        ooff = sl * a.oslab + (b - sl * a.batch) * a.odist;
+      }
+      c.gout = reinterpret_cast<V *>(a.out) + ooff;
+      V v[EMAX];
+      constexpr int R = S.rad[0];
+      constexpr int B = L / R;
+      constexpr int K = (B + P - 1) / P;
+      constexpr bool FULL = (B % P) == 0;
+#pragma unroll
+      for (int i = 0; i < K; ++i) {
+        const int j = c.g + P * i;
+        if (FULL || j < B) {
+#pragma unroll
+          for (int r = 0; r < R; ++r)
+            v[i * R + r] = c.sm[sidx(c, j + r * B)];
+        }
+      }
+      run<0>(c, v);
+      __syncthreads(); // this buffer is refilled two tiles from now
+      tile = next;
+      if (tile >= ntiles)
+        break;
+    }
   }
 };
 
@@ -356,6 +490,14 @@ __global__ void __launch_bounds__(NT)
   using K = KS<T, L, NT, TB, COL, FWD, KIND>;
   extern __shared__ __align__(16) unsigned char smraw[];
   K::entry(a, reinterpret_cast<typename K::V *>(smraw));
+}
+
+template <typename T, int L, int NT, int TB, bool FWD>
+__global__ void __launch_bounds__(NT)
+    fft_static_staged_kernel(const PassArgs a) {
+  using K = KS<T, L, NT, TB, true, FWD, KIND_C2C, true>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  K::entry_staged(a, reinterpret_cast<typename K::V *>(smraw));
 }
 
 // ==========================================================================
@@ -371,11 +513,10 @@ BF_D void gen_butterfly(const GenArgs &a, const V *A, V *Bm, const V *tw,
                         int tb, int j, int k, int Bq, int Ns, int texp) {
   V v[R];
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
+  for (int r = 0; r < R; ++r)
     v[r] = A[gidx<COL>(tb, j + r * Bq, a.TB, a.L)];
-    if (r > 0 && Ns > 1)
-      v[r] = cmulw<!FWD>(v[r], ldtw(tw, r * k * texp * a.tscale));
-  }
+  if (Ns > 1)
+    apply_twiddles<R, !FWD>(v, tw, k * texp * a.tscale);
   dft<R, FWD>(v);
   const int base = (j - k) * R + k; // (j/Ns)*Ns*R + k
 #pragma unroll

@@ -46,9 +46,9 @@ __global__ void twiddle_table_kernel(double2 *t64, float2 *t32, int n) {
 
 namespace {
 
-template <typename T> constexpr size_t smem_s(int L, bool col) {
-  const CfgS c = cfg_static(static_cast<int>(sizeof(cvec<T>)), L, col);
-  const int LP = col ? L : (L + L / 8);
+template <typename T> constexpr size_t smem_s(int L, bool col, int var) {
+  const CfgS c = cfg_static(static_cast<int>(sizeof(cvec<T>)), L, col, var);
+  const int LP = col ? L : (L + (L >> (sizeof(cvec<T>) == 8 ? 4 : 3)));
   return static_cast<size_t>(c.TB) * LP * sizeof(cvec<T>);
 }
 
@@ -102,10 +102,10 @@ size_t generic_smem_bytes(bool f64, int TB, int L) {
   return 2ull * TB * L * (f64 ? sizeof(double2) : sizeof(float2));
 }
 
-size_t static_smem_bytes(int esize_complex, int L, bool col) {
+size_t static_smem_bytes(int esize_complex, int L, bool col, int var) {
   if (!static_length_ok(L))
     return 0;
-  return esize_complex == 16 ? smem_s<double>(L, col) : smem_s<float>(L, col);
+  return esize_complex == 16 ? smem_s<double>(L, col, var) : smem_s<float>(L, col, var);
 }
 
 cudaError_t launch_twiddle_table(double2 *t64, float2 *t32, int n,

@@ -2,12 +2,12 @@
 #include "fs_launch.cuh"
 
 namespace b200fft {
-cudaError_t launch_static_c2c_f32(int L, bool col, bool fwd, const PassArgs &a,
+cudaError_t launch_static_c2c_f32(int L, bool col, bool fwd, int var, const PassArgs &a,
                                   cudaStream_t st) {
   if (col)
-    return fwd ? launch_static_switch<float, true, true, KIND_C2C>(L, a, st)
-               : launch_static_switch<float, true, false, KIND_C2C>(L, a, st);
-  return fwd ? launch_static_switch<float, false, true, KIND_C2C>(L, a, st)
-             : launch_static_switch<float, false, false, KIND_C2C>(L, a, st);
+    return fwd ? launch_static_switch<float, true, true, KIND_C2C>(L, var, a, st)
+               : launch_static_switch<float, true, false, KIND_C2C>(L, var, a, st);
+  return fwd ? launch_static_switch<float, false, true, KIND_C2C>(L, var, a, st)
+             : launch_static_switch<float, false, false, KIND_C2C>(L, var, a, st);
 }
 } // namespace b200fft

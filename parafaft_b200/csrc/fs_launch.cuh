@@ -10,9 +10,9 @@
 
 namespace b200fft {
 
-template <typename T, int L, bool COL, bool FWD, int KIND>
+template <typename T, int L, bool COL, bool FWD, int KIND, int VAR>
 cudaError_t launch_static_one(const PassArgs &a, cudaStream_t st) {
-  constexpr CfgS cf = cfg_static(static_cast<int>(sizeof(cvec<T>)), L, COL);
+  constexpr CfgS cf = cfg_static(static_cast<int>(sizeof(cvec<T>)), L, COL, VAR);
   using K = KS<T, L, cf.NT, cf.TB, COL, FWD, KIND>;
   auto kern = fft_static_kernel<T, L, cf.NT, cf.TB, COL, FWD, KIND>;
   constexpr size_t smem = K::smem_bytes();
@@ -38,26 +38,78 @@ cudaError_t launch_static_one(const PassArgs &a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-#define B2_FS_CASES(T, COL, FWD, KIND)                                          \
-  case 2: return launch_static_one<T, 2, COL, FWD, KIND>(a, st);              \
-  case 4: return launch_static_one<T, 4, COL, FWD, KIND>(a, st);              \
-  case 8: return launch_static_one<T, 8, COL, FWD, KIND>(a, st);              \
-  case 16: return launch_static_one<T, 16, COL, FWD, KIND>(a, st);            \
-  case 32: return launch_static_one<T, 32, COL, FWD, KIND>(a, st);            \
-  case 64: return launch_static_one<T, 64, COL, FWD, KIND>(a, st);            \
-  case 128: return launch_static_one<T, 128, COL, FWD, KIND>(a, st);          \
-  case 256: return launch_static_one<T, 256, COL, FWD, KIND>(a, st);          \
-  case 512: return launch_static_one<T, 512, COL, FWD, KIND>(a, st);          \
-  case 1024: return launch_static_one<T, 1024, COL, FWD, KIND>(a, st);        \
-  case 2048: return launch_static_one<T, 2048, COL, FWD, KIND>(a, st);
+inline int sm_count() {
+  static int n[32] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 32)
+    dev = 0;
+  if (n[dev] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    n[dev] = v;
+  }
+  return n[dev];
+}
+
+template <typename T, int L, bool FWD>
+cudaError_t launch_static_staged(const PassArgs &a, cudaStream_t st) {
+  constexpr CfgS cf = cfg_static(static_cast<int>(sizeof(cvec<T>)), L, true, kVariantStaged);
+  using K = KS<T, L, cf.NT, cf.TB, true, FWD, KIND_C2C, true>;
+  auto kern = fft_static_staged_kernel<T, L, cf.NT, cf.TB, FWD>;
+  constexpr size_t smem = K::smem_bytes();
+  static int configured_mask = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (smem > 48 * 1024 && dev >= 0 && dev < 31 && !(configured_mask & (1 << dev))) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess)
+      return e;
+    configured_mask |= (1 << dev);
+  }
+  const long long ntiles = (a.total + cf.TB - 1) / cf.TB;
+  if (ntiles <= 0)
+    return cudaSuccess;
+  const int per_sm = smem <= 100 * 1024 ? 2 : 1;
+  const long long grid = ntiles < static_cast<long long>(sm_count()) * per_sm
+                             ? ntiles
+                             : static_cast<long long>(sm_count()) * per_sm;
+  kern<<<static_cast<unsigned>(grid), cf.NT, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T, int L, bool COL, bool FWD, int KIND>
+cudaError_t launch_static_var(int var, const PassArgs &a, cudaStream_t st) {
+  if constexpr (COL && KIND == KIND_C2C) {
+    if (var == kVariantStaged)
+      return launch_static_staged<T, L, FWD>(a, st);
+  }
+  switch (var) {
+  case 1: return launch_static_one<T, L, COL, FWD, KIND, 1>(a, st);
+  case 2: return launch_static_one<T, L, COL, FWD, KIND, 2>(a, st);
+  case 3:
+    if constexpr (COL)
+      return launch_static_one<T, L, COL, FWD, KIND, 3>(a, st);
+    else
+      return launch_static_one<T, L, COL, FWD, KIND, 0>(a, st);
+  default: return launch_static_one<T, L, COL, FWD, KIND, 0>(a, st);
+  }
+}
+
+#define B2_FS_CASE(LL)                                                         \
+  case LL: return launch_static_var<T, LL, COL, FWD, KIND>(var, a, st);
 
 template <typename T, bool COL, bool FWD, int KIND>
-cudaError_t launch_static_switch(int L, const PassArgs &a, cudaStream_t st) {
+cudaError_t launch_static_switch(int L, int var, const PassArgs &a, cudaStream_t st) {
   switch (L) {
-    B2_FS_CASES(T, COL, FWD, KIND)
+    B2_FS_CASE(2) B2_FS_CASE(4) B2_FS_CASE(8) B2_FS_CASE(16) B2_FS_CASE(32)
+    B2_FS_CASE(64) B2_FS_CASE(128) B2_FS_CASE(256) B2_FS_CASE(512)
+    B2_FS_CASE(1024) B2_FS_CASE(2048)
   case 4096:
     if constexpr (KIND == KIND_C2C)
-      return launch_static_one<T, 4096, COL, FWD, KIND>(a, st);
+      return launch_static_var<T, 4096, COL, FWD, KIND>(var, a, st);
     else
       return cudaErrorInvalidValue;
   default:

@@ -2,10 +2,10 @@
 #include "fs_launch.cuh"
 
 namespace b200fft {
-cudaError_t launch_static_r2c_f32(int L, const PassArgs &a, cudaStream_t st) {
-  return launch_static_switch<float, false, true, KIND_R2C>(L, a, st);
+cudaError_t launch_static_r2c_f32(int L, int var, const PassArgs &a, cudaStream_t st) {
+  return launch_static_switch<float, false, true, KIND_R2C>(L, var, a, st);
 }
-cudaError_t launch_static_c2r_f32(int L, const PassArgs &a, cudaStream_t st) {
-  return launch_static_switch<float, false, false, KIND_C2R>(L, a, st);
+cudaError_t launch_static_c2r_f32(int L, int var, const PassArgs &a, cudaStream_t st) {
+  return launch_static_switch<float, false, false, KIND_C2R>(L, var, a, st);
 }
 } // namespace b200fft

@@ -9,19 +9,19 @@ namespace b200fft {
 
 // Family S: specialised kernels for power-of-two stage lengths L.
 // C2C: col selects the column thread mapping (strided points).
-cudaError_t launch_static_c2c_f32(int L, bool col, bool fwd, const PassArgs &a,
+cudaError_t launch_static_c2c_f32(int L, bool col, bool fwd, int var, const PassArgs &a,
                                   cudaStream_t st);
-cudaError_t launch_static_c2c_f64(int L, bool col, bool fwd, const PassArgs &a,
+cudaError_t launch_static_c2c_f64(int L, bool col, bool fwd, int var, const PassArgs &a,
                                   cudaStream_t st);
 // R2C (forward) / C2R (backward) of real length 2L, contiguous padded rows;
 // both sides of `a` in complex units.
-cudaError_t launch_static_r2c_f32(int L, const PassArgs &a, cudaStream_t st);
-cudaError_t launch_static_c2r_f32(int L, const PassArgs &a, cudaStream_t st);
-cudaError_t launch_static_r2c_f64(int L, const PassArgs &a, cudaStream_t st);
-cudaError_t launch_static_c2r_f64(int L, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_static_r2c_f32(int L, int var, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_static_c2r_f32(int L, int var, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_static_r2c_f64(int L, int var, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_static_c2r_f64(int L, int var, const PassArgs &a, cudaStream_t st);
 
 // Shared-memory bytes of a Family S launch (0 when no kernel exists).
-size_t static_smem_bytes(int esize_complex, int L, bool col);
+size_t static_smem_bytes(int esize_complex, int L, bool col, int var);
 
 // Family G: runtime-generic kernels.
 cudaError_t launch_generic(bool f64, int kind, bool col, bool fwd,

@@ -242,3 +242,16 @@ def test_partial_copy_coverage(prec):
     ref[3:7] = np.fft.fft(ref[3:7], axis=1)
     assert O.rel_l2(y, ref) < tol(prec)
     assert h.stats()["fused_copies"] == 1
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("length", [2, 8, 64, 512, 1024, 4096])
+def test_tile_variants(prec, variant, length, monkeypatch):
+    """Every tile-shape candidate the planner can pick computes the same
+    transform, for column and row layouts, in place and fused out of place."""
+    monkeypatch.setenv("B200FFT_VARIANT", str(variant))
+    batch = max(5, 40000 // length) + 3
+    for stride, dist in ((batch, 1), (1, length)):
+        y, ref, h = _c2c_case(prec, length, batch, stride, dist, nv.BACKWARD, seed=variant)
+        assert O.rel_l2(y, ref) < tol(prec), (variant, length, stride)
