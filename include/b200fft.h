@@ -153,6 +153,22 @@ int b200fft_flush(b200fft_handle h);
 int b200fft_alloc(size_t bytes, void **ptr);
 int b200fft_free(void *ptr);
 
+/* ---- transform without allocation (no counterpart in the reference) ------ */
+/* One batched C2C transform of `length` points (element j of transform b at
+ * in/out[b*dist + j*stride], in == out allowed) on `cuda_stream` (NULL: the
+ * default stream), for callers that cannot allocate device memory where they
+ * transform: applications that hand out all device memory from their own pool,
+ * and latency-critical loops that must not let cudaMalloc/cudaFree synchronize
+ * the device. It needs no handle and calls no allocator: its twiddle table
+ * lives in a fixed 64 KiB array inside the library, so `length` must be a
+ * power of two from 2 to 4096 (anything else returns B200FFT_ERR_UNSUPPORTED).
+ * The first call on a device resolves that array's address; make it before any
+ * stream capture. All calls on a device share the array: calls that may run
+ * concurrently on the GPU race, so order them on one stream. */
+int b200fft_c2c_noalloc(int precision, int direction, int length, size_t batch,
+                        ptrdiff_t stride, ptrdiff_t dist, const void *in, void *out,
+                        void *cuda_stream);
+
 /* ---- introspection ------------------------------------------------------ */
 int b200fft_get_stats(b200fft_handle h, b200fft_stats *out);
 int b200fft_reset_stats(b200fft_handle h);

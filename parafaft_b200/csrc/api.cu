@@ -249,6 +249,12 @@ std::mutex g_alloc_mu;
 
 } // namespace
 
+namespace b200fft {
+// Lets other translation units of the library report through
+// b200fft_last_error().
+void set_error_text(const std::string &msg) { g_err = msg; }
+} // namespace b200fft
+
 struct b200fft_handle_s {
   int prec = B200FFT_F32;
   int rsize = 4; // bytes of FloatType

@@ -37,7 +37,7 @@ ENGINE_SYMBOLS = (
     "b200fft_plan_c2r", "b200fft_exec_c2r", "b200fft_memcpy", "b200fft_memcpy2d",
     "b200fft_sync", "b200fft_flush", "b200fft_alloc", "b200fft_free",
     "b200fft_get_stats", "b200fft_reset_stats", "b200fft_get_log", "b200fft_set_profiling",
-    "b200fft_describe", "b200fft_supported",
+    "b200fft_describe", "b200fft_supported", "b200fft_c2c_noalloc",
 )
 
 
@@ -105,6 +105,7 @@ def engine() -> C.CDLL:
             "b200fft_set_profiling": (i, [vp, i]),
             "b200fft_describe": (i, [i, i, i, sz, pd, pd, C.c_char_p, sz]),
             "b200fft_supported": (i, [i, i, i]),
+            "b200fft_c2c_noalloc": (i, [i, i, i, sz, pd, pd, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -254,6 +255,14 @@ def describe(precision: int, kind: int, length: int, batch: int = 1, stride: int
     buf = C.create_string_buffer(256)
     check(engine().b200fft_describe(precision, kind, length, batch, stride, dist, buf, 256))
     return buf.value.decode()
+
+
+def c2c_noalloc(precision: int, direction: int, length: int, batch: int, stride: int,
+                dist: int, data_in, data_out, stream: int | None = None) -> None:
+    """b200fft_c2c_noalloc: one batched C2C transform without a handle and
+    without any device allocation (power-of-two lengths up to 4096)."""
+    check(engine().b200fft_c2c_noalloc(precision, direction, length, batch, stride, dist,
+                                       _ptr(data_in), _ptr(data_out), stream or 0))
 
 
 def supported(precision: int, kind: int, length: int) -> bool:
