@@ -153,6 +153,34 @@ int b200fft_flush(b200fft_handle h);
 int b200fft_alloc(size_t bytes, void **ptr);
 int b200fft_free(void *ptr);
 
+/* ---- batches of independent grids (no counterpart in the reference: the
+ *      batching extension of the backend) ---------------------------------- */
+/* A group runs the transforms of many handles (for example one ParaFaFT
+ * object per grid) together. Member handles use the group's stream. Between
+ * b200fft_group_begin and b200fft_group_end their passes are recorded (after
+ * the usual copy fusion and slice coalescing) instead of launched, and
+ * b200fft_sync on them returns at once. b200fft_group_end then runs the
+ * recording: the d-th recorded pass of every handle forms one persistent
+ * launch whose CTAs take (transform, tile) work items from a device queue.
+ * The recorded schedule stays valid for the same buffers: group_replay runs
+ * it again, group_capture records it once into a CUDA graph that replay then
+ * launches. */
+typedef struct b200fft_group_s *b200fft_group;
+int b200fft_group_create(b200fft_group *out);
+/* Detaches the member handles (they return to their own streams). */
+int b200fft_group_destroy(b200fft_group g);
+int b200fft_group_add(b200fft_group g, b200fft_handle h);
+int b200fft_group_begin(b200fft_group g);
+/* Build the schedule from the recording and run it once (asynchronously). */
+int b200fft_group_end(b200fft_group g);
+/* Record the built schedule into a CUDA graph (replay then launches it). */
+int b200fft_group_capture(b200fft_group g);
+/* Run the built schedule again on the group's stream. */
+int b200fft_group_replay(b200fft_group g);
+int b200fft_group_sync(b200fft_group g);
+/* Launches, passes and bytes of the last built schedule. */
+int b200fft_group_stats(b200fft_group g, b200fft_stats *out);
+
 /* ---- transform without allocation (no counterpart in the reference) ------ */
 /* One batched C2C transform of `length` points (element j of transform b at
  * in/out[b*dist + j*stride], in == out allowed) on `cuda_stream` (NULL: the
@@ -160,7 +188,7 @@ int b200fft_free(void *ptr);
  * transform: applications that hand out all device memory from their own pool,
  * and latency-critical loops that must not let cudaMalloc/cudaFree synchronize
  * the device. It needs no handle and calls no allocator: its twiddle table
- * lives in a fixed 64 KiB array inside the library, so `length` must be a
+ * lives in a fixed 128 KiB array inside the library, so `length` must be a
  * power of two from 2 to 4096 (anything else returns B200FFT_ERR_UNSUPPORTED).
  * The first call on a device resolves that array's address; make it before any
  * stream capture. All calls on a device share the array: calls that may run

@@ -87,6 +87,21 @@ struct HeldCopy {
   size_t bytes = 0;
 };
 
+// An operation recorded while the handle is inside a group.
+struct RecOp {
+  enum { PASS = 0, COPY = 1, COPY2D = 2 };
+  int type = PASS;
+  Plan plan;
+  int dir = 0;
+  const void *in = nullptr;
+  void *out = nullptr;
+  const void *tw = nullptr;
+  long long slabs = 1, slab = 0;
+  void *dst = nullptr;
+  const void *src = nullptr;
+  size_t bytes = 0, dpitch = 0, spitch = 0, width = 0, height = 0;
+};
+
 struct HeldRun {
   bool active = false;
   int stage = -1;
@@ -284,8 +299,47 @@ struct b200fft_handle_s {
   std::vector<cudaEvent_t> event_pool;
   size_t seq = 0;        // sequence number of the next log record
   size_t log_base = 0;   // sequence number of log.front()
+  // group membership (b200fft_group_*)
+  b200fft_group_s *group = nullptr;
+  bool recording = false;
+  std::vector<RecOp> recs;
 
   size_t csize() const { return 2 * static_cast<size_t>(rsize); }
+};
+
+namespace {
+
+struct GroupStep {
+  enum { PASSES = 0, COPY = 1, COPY2D = 2 };
+  int type = PASSES;
+  // grouped generic pass
+  bool f64 = false, col = false, fwd = true;
+  int kind = KIND_C2C;
+  std::vector<GenArgs> items;
+  std::vector<long long> tile_start;
+  GenArgs *d_items = nullptr;
+  long long *d_tile_start = nullptr;
+  size_t smem = 0;
+  int grid = 0;
+  int queue = 0;
+  long long bytes = 0;
+  // copy
+  RecOp op;
+};
+
+} // namespace
+
+struct b200fft_group_s {
+  std::vector<b200fft_handle_s *> handles;
+  cudaStream_t stream = nullptr;
+  bool record_only = false;
+  bool recording = false;
+  std::vector<GroupStep> steps;
+  unsigned long long *d_queues = nullptr;
+  int nqueues = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  b200fft_stats stats{};
 };
 
 namespace {
@@ -371,7 +425,7 @@ int get_table(H *h, int n, const void **out) {
     return B200FFT_SUCCESS;
   }
   void *p = nullptr;
-  cudaError_t e = cudaMalloc(&p, static_cast<size_t>(n) * h->csize());
+  cudaError_t e = cudaMalloc(&p, static_cast<size_t>(twiddle_table_entries(n)) * h->csize());
   if (e != cudaSuccess)
     return cuda_fail(e, "cudaMalloc (twiddle table)");
   if (h->prec == B200FFT_F64)
@@ -433,6 +487,15 @@ bool overlaps(const char *a, size_t na, const char *b, size_t nb) {
 int issue_copy(H *h, void *dst, const void *src, size_t bytes) {
   if (bytes == 0 || dst == src)
     return B200FFT_SUCCESS;
+  if (h->recording) {
+    RecOp op;
+    op.type = RecOp::COPY;
+    op.dst = dst;
+    op.src = src;
+    op.bytes = bytes;
+    h->recs.push_back(op);
+    return B200FFT_SUCCESS;
+  }
   h->stats.copies_issued++;
   h->stats.bytes_copied += bytes;
   b200fft_launch_record r{};
@@ -476,42 +539,64 @@ int finish_fused_copy(H *h, const char *out0, size_t covered) {
 
 // Launch one pass of plan p. `in`/`out` point at the first transform;
 // slabs/slab (complex elements) describe a coalesced middle-axis run.
-int launch_pass(H *h, const Plan &p, int dir, const void *in, void *out,
-                long long slabs, long long slab, bool fused, int stage) {
-  const void *tw = nullptr;
-  B2_TRY(get_table(h, p.ch.tlen, &tw));
+// Kernel arguments of one pass of plan p run by kernel family `family`
+// (element units differ between the specialised and generic R2C/C2R kernels).
+PassArgs pass_args(const Plan &p, int family, const void *in, void *out, const void *tw,
+                   long long slabs, long long slab) {
   PassArgs a{};
   a.in = in;
   a.out = out;
   a.tw = tw;
   a.batch = p.batch;
   a.total = p.batch * slabs;
-  long long bytes = 0;
-  const long long cs = static_cast<long long>(h->csize());
-  const long long rs = h->rsize;
   if (p.kind == KIND_C2C) {
     a.idist = a.odist = p.dist;
     a.istride = a.ostride = p.stride;
     a.islab = a.oslab = slab;
-    bytes = 2LL * a.total * p.len * cs;
+  } else if (family == 0) { // both sides complex units, contiguous rows
+    a.idist = a.odist = p.dist / 2;
+    a.istride = a.ostride = 1;
+    a.islab = a.oslab = 0;
+  } else if (p.kind == KIND_R2C) {
+    a.idist = p.dist;
+    a.istride = p.stride;
+    a.odist = p.dist / 2;
+    a.ostride = p.stride;
   } else {
-    const long long nc = p.len / 2 + 1;
-    bytes = a.total * (p.len * rs + nc * cs);
-    if (p.ch.family == 0) { // both sides complex units, contiguous rows
-      a.idist = a.odist = p.dist / 2;
-      a.istride = a.ostride = 1;
-      a.islab = a.oslab = 0;
-    } else if (p.kind == KIND_R2C) {
-      a.idist = p.dist;
-      a.istride = p.stride;
-      a.odist = p.dist / 2;
-      a.ostride = p.stride;
-    } else {
-      a.idist = p.dist / 2;
-      a.istride = p.stride;
-      a.odist = p.dist;
-      a.ostride = p.stride;
-    }
+    a.idist = p.dist / 2;
+    a.istride = p.stride;
+    a.odist = p.dist;
+    a.ostride = p.stride;
+  }
+  return a;
+}
+
+long long pass_bytes(const H *h, const Plan &p, long long total) {
+  const long long cs = static_cast<long long>(h->csize());
+  if (p.kind == KIND_C2C)
+    return 2LL * total * p.len * cs;
+  return total * (p.len * static_cast<long long>(h->rsize) + (p.len / 2 + 1) * cs);
+}
+
+int launch_pass(H *h, const Plan &p, int dir, const void *in, void *out,
+                long long slabs, long long slab, bool fused, int stage) {
+  const void *tw = nullptr;
+  B2_TRY(get_table(h, p.ch.tlen, &tw));
+  PassArgs a = pass_args(p, p.ch.family, in, out, tw, slabs, slab);
+  const long long bytes = pass_bytes(h, p, a.total);
+  if (h->recording) { // inside a group: the group launches it later
+    RecOp op;
+    op.type = RecOp::PASS;
+    op.plan = p;
+    op.dir = dir;
+    op.in = in;
+    op.out = out;
+    op.tw = tw;
+    op.slabs = slabs;
+    op.slab = slab;
+    h->recs.push_back(op);
+    h->stats.bytes_transformed += static_cast<uint64_t>(bytes);
+    return B200FFT_SUCCESS;
   }
   h->stats.kernel_launches++;
   h->stats.bytes_transformed += static_cast<uint64_t>(bytes);
@@ -731,7 +816,16 @@ int b200fft_create(int precision, int num_stages, int plan_flag, unsigned flags,
 int b200fft_destroy(b200fft_handle h) {
   if (h == nullptr)
     return B200FFT_SUCCESS;
+  h->recording = false;
   int rc = flush_all(h);
+  if (h->group != nullptr) { // leave the group first
+    auto &v = h->group->handles;
+    v.erase(std::remove(v.begin(), v.end(), h), v.end());
+    if (!h->record_only && h->stream)
+      cudaStreamSynchronize(h->stream);
+    h->group = nullptr;
+    h->stream = h->own;
+  }
   if (!h->record_only) {
     if (h->stream)
       cudaStreamSynchronize(h->stream);
@@ -862,6 +956,18 @@ int b200fft_memcpy2d(b200fft_handle h, void *dst, size_t dpitch, const void *src
   B2_TRY(flush_all(h));
   if (width == 0 || height == 0)
     return B200FFT_SUCCESS;
+  if (h->recording) {
+    RecOp op;
+    op.type = RecOp::COPY2D;
+    op.dst = dst;
+    op.src = src;
+    op.dpitch = dpitch;
+    op.spitch = spitch;
+    op.width = width;
+    op.height = height;
+    h->recs.push_back(op);
+    return B200FFT_SUCCESS;
+  }
   h->stats.copies_issued++;
   h->stats.bytes_copied += width * height;
   b200fft_launch_record r{};
@@ -891,7 +997,7 @@ int b200fft_flush(b200fft_handle h) {
 int b200fft_sync(b200fft_handle h) {
   B2_TRY(check_handle(h));
   B2_TRY(flush_all(h));
-  if (h->record_only)
+  if (h->record_only || h->recording) // inside a group: b200fft_group_sync waits
     return B200FFT_SUCCESS;
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess)
@@ -994,6 +1100,340 @@ int b200fft_supported(int precision, int kind, int length) {
   const int rc = choose_kernel(precision, kind, length, 1, 1, kind == KIND_C2C ? length : 2 * (length / 2 + 1), false, &ch);
   g_err = keep;
   return rc == B200FFT_SUCCESS ? 1 : 0;
+}
+
+} // extern "C"
+
+// ============================================================================
+// Groups: many handles transformed together (independent grids).
+// ============================================================================
+namespace {
+
+using G = b200fft_group_s;
+
+void group_free_schedule(G *g) {
+  if (g->gexec)
+    cudaGraphExecDestroy(g->gexec);
+  if (g->graph)
+    cudaGraphDestroy(g->graph);
+  g->gexec = nullptr;
+  g->graph = nullptr;
+  if (!g->record_only) {
+    for (GroupStep &s : g->steps) {
+      if (s.d_items)
+        cudaFree(s.d_items);
+      if (s.d_tile_start)
+        cudaFree(s.d_tile_start);
+    }
+    if (g->d_queues)
+      cudaFree(g->d_queues);
+  }
+  g->d_queues = nullptr;
+  g->nqueues = 0;
+  g->steps.clear();
+}
+
+int sm_count_current() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    n = 148;
+  }
+  return n;
+}
+
+// Build the steps of the schedule from the members' recordings.
+int group_build(G *g) {
+  group_free_schedule(g);
+  size_t depth = 0;
+  for (H *h : g->handles)
+    depth = std::max(depth, h->recs.size());
+  for (size_t d = 0; d < depth; ++d) {
+    std::map<int, size_t> bucket; // (f64, kind, col, fwd) -> step index
+    for (H *h : g->handles) {
+      if (d >= h->recs.size())
+        continue;
+      const RecOp &op = h->recs[d];
+      if (op.type != RecOp::PASS) {
+        GroupStep s;
+        s.type = op.type == RecOp::COPY ? GroupStep::COPY : GroupStep::COPY2D;
+        s.op = op;
+        g->steps.push_back(s);
+        continue;
+      }
+      const Plan &p = op.plan;
+      Choice gc;
+      B2_TRY(choose_kernel(h->prec, p.kind, p.len, p.batch, p.stride, p.dist, true, &gc));
+      GenArgs ga = gc.gen;
+      ga.p = pass_args(p, 1, op.in, op.out, op.tw, op.slabs, op.slab);
+      const bool f64 = h->prec == B200FFT_F64;
+      const bool fwd = op.dir == B200FFT_FORWARD;
+      const int key = (f64 ? 1 : 0) | (p.kind << 1) | ((gc.col ? 1 : 0) << 3) | ((fwd ? 1 : 0) << 4);
+      auto it = bucket.find(key);
+      size_t si;
+      if (it == bucket.end()) {
+        GroupStep s;
+        s.type = GroupStep::PASSES;
+        s.f64 = f64;
+        s.kind = p.kind;
+        s.col = gc.col;
+        s.fwd = fwd;
+        s.tile_start.push_back(0);
+        g->steps.push_back(s);
+        si = g->steps.size() - 1;
+        bucket[key] = si;
+      } else {
+        si = it->second;
+      }
+      GroupStep &s = g->steps[si];
+      const long long tiles = (ga.p.total + ga.TB - 1) / ga.TB;
+      s.items.push_back(ga);
+      s.tile_start.push_back(s.tile_start.back() + tiles);
+      s.smem = std::max(s.smem, generic_smem_bytes(f64, ga.TB, ga.L));
+      s.bytes += pass_bytes(h, p, ga.p.total);
+    }
+  }
+  // device copies of the work lists, one queue counter per grouped launch
+  int q = 0;
+  for (GroupStep &s : g->steps)
+    if (s.type == GroupStep::PASSES)
+      s.queue = q++;
+  g->nqueues = q;
+  if (g->record_only)
+    return B200FFT_SUCCESS;
+  const int sms = sm_count_current();
+  for (GroupStep &s : g->steps) {
+    if (s.type != GroupStep::PASSES)
+      continue;
+    cudaError_t e = cudaMalloc(&s.d_items, s.items.size() * sizeof(GenArgs));
+    if (e == cudaSuccess)
+      e = cudaMalloc(&s.d_tile_start, s.tile_start.size() * sizeof(long long));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(s.d_items, s.items.data(), s.items.size() * sizeof(GenArgs),
+                     cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(s.d_tile_start, s.tile_start.data(),
+                     s.tile_start.size() * sizeof(long long), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "group work list upload");
+    const int per_sm = std::max<int>(1, std::min<int>(8, static_cast<int>(
+                                             (227 * 1024) / (s.smem + 1024))));
+    const long long tasks = s.tile_start.back();
+    s.grid = static_cast<int>(std::min<long long>(tasks, static_cast<long long>(sms) * per_sm));
+  }
+  if (q > 0) {
+    cudaError_t e = cudaMalloc(&g->d_queues, q * sizeof(unsigned long long));
+    if (e != cudaSuccess)
+      return cuda_fail(e, "group queue counters");
+  }
+  return B200FFT_SUCCESS;
+}
+
+int group_run(G *g) {
+  g->stats.exec_calls++;
+  for (GroupStep &s : g->steps) {
+    if (s.type == GroupStep::PASSES) {
+      g->stats.kernel_launches++;
+      g->stats.bytes_transformed += static_cast<uint64_t>(s.bytes);
+    } else {
+      g->stats.copies_issued++;
+    }
+  }
+  if (g->record_only)
+    return B200FFT_SUCCESS;
+  cudaGetLastError(); // report only errors of the calls below
+  for (size_t i = 0; i < g->steps.size(); ++i) {
+    GroupStep &s = g->steps[i];
+    cudaError_t e = cudaSuccess;
+    const char *what = "grouped pass";
+    if (s.type == GroupStep::PASSES) {
+      if (s.tile_start.back() == 0)
+        continue;
+      e = cudaMemsetAsync(g->d_queues + s.queue, 0, sizeof(unsigned long long), g->stream);
+      if (e != cudaSuccess)
+        what = "queue reset";
+      else
+        e = launch_generic_group(s.f64, s.kind, s.col, s.fwd, s.d_items, s.d_tile_start,
+                                 static_cast<int>(s.items.size()), g->d_queues + s.queue,
+                                 s.smem, s.grid, g->stream);
+    } else if (s.type == GroupStep::COPY) {
+      what = "copy";
+      e = cudaMemcpyAsync(s.op.dst, s.op.src, s.op.bytes, cudaMemcpyDefault, g->stream);
+    } else {
+      what = "2D copy";
+      e = cudaMemcpy2DAsync(s.op.dst, s.op.dpitch, s.op.src, s.op.spitch, s.op.width,
+                            s.op.height, cudaMemcpyDefault, g->stream);
+    }
+    if (e != cudaSuccess) {
+      char buf[160];
+      std::snprintf(buf, sizeof(buf), "group step %zu (%s, kind %d, %zu items, grid %d, smem %zu)",
+                    i, what, s.kind, s.items.size(), s.grid, s.smem);
+      return cuda_fail(e, buf);
+    }
+  }
+  return B200FFT_SUCCESS;
+}
+
+} // namespace
+
+extern "C" {
+
+int b200fft_group_create(b200fft_group *out) {
+  if (out == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_create: null output");
+  *out = nullptr;
+  G *g = new G();
+  g->record_only = env_flag("B200FFT_RECORD_ONLY");
+  if (!g->record_only) {
+    cudaError_t e = cudaStreamCreate(&g->stream);
+    if (e != cudaSuccess) {
+      delete g;
+      return cuda_fail(e, "cudaStreamCreate (group)");
+    }
+  }
+  *out = g;
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_group_destroy(b200fft_group g) {
+  if (g == nullptr)
+    return B200FFT_SUCCESS;
+  if (!g->record_only && g->stream)
+    cudaStreamSynchronize(g->stream);
+  for (H *h : g->handles) {
+    h->recording = false;
+    h->recs.clear();
+    h->group = nullptr;
+    h->stream = h->own;
+  }
+  group_free_schedule(g);
+  if (!g->record_only && g->stream)
+    cudaStreamDestroy(g->stream);
+  delete g;
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_group_add(b200fft_group g, b200fft_handle h) {
+  if (g == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_add: null group");
+  B2_TRY(check_handle(h));
+  if (h->group != nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_add: handle already in a group");
+  if (h->record_only != g->record_only)
+    return fail(B200FFT_ERR_INVALID_ARG,
+                "b200fft_group_add: record-only and device handles cannot share a group");
+  B2_TRY(flush_all(h));
+  if (!h->record_only) {
+    // work already queued on the handle's stream finishes before group work
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "cudaStreamSynchronize (group_add)");
+    h->stream = g->stream;
+  }
+  h->group = g;
+  g->handles.push_back(h);
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_group_begin(b200fft_group g) {
+  if (g == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_begin: null group");
+  if (g->recording)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_begin: already recording");
+  for (H *h : g->handles) {
+    B2_TRY(flush_all(h));
+    h->recs.clear();
+    h->recording = true;
+  }
+  g->recording = true;
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_group_end(b200fft_group g) {
+  if (g == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_end: null group");
+  if (!g->recording)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_end: group_begin was not called");
+  int rc = B200FFT_SUCCESS;
+  for (H *h : g->handles) {
+    const int r = flush_all(h);
+    if (rc == B200FFT_SUCCESS)
+      rc = r;
+    h->recording = false;
+  }
+  g->recording = false;
+  if (rc == B200FFT_SUCCESS)
+    rc = group_build(g);
+  for (H *h : g->handles)
+    h->recs.clear();
+  B2_TRY(rc);
+  return group_run(g);
+}
+
+int b200fft_group_capture(b200fft_group g) {
+  if (g == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_capture: null group");
+  if (g->record_only)
+    return B200FFT_SUCCESS;
+  if (g->gexec) {
+    cudaGraphExecDestroy(g->gexec);
+    g->gexec = nullptr;
+  }
+  if (g->graph) {
+    cudaGraphDestroy(g->graph);
+    g->graph = nullptr;
+  }
+  cudaError_t e = cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaStreamBeginCapture");
+  const b200fft_stats keep = g->stats;
+  const int rc = group_run(g);
+  g->stats = keep;
+  e = cudaStreamEndCapture(g->stream, &g->graph);
+  if (rc != B200FFT_SUCCESS)
+    return rc;
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&g->gexec, g->graph, 0);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaGraphInstantiate");
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_group_replay(b200fft_group g) {
+  if (g == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_replay: null group");
+  if (g->gexec == nullptr)
+    return group_run(g);
+  g->stats.exec_calls++;
+  cudaError_t e = cudaGraphLaunch(g->gexec, g->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaGraphLaunch");
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_group_sync(b200fft_group g) {
+  if (g == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_sync: null group");
+  if (g->record_only)
+    return B200FFT_SUCCESS;
+  cudaError_t e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaStreamSynchronize (group)");
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_group_stats(b200fft_group g, b200fft_stats *out) {
+  if (g == nullptr || out == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_stats: null argument");
+  *out = g->stats;
+  size_t passes = 0;
+  for (const GroupStep &s : g->steps)
+    passes += s.items.size();
+  out->exec_calls = g->stats.exec_calls;
+  out->coalesced_calls = passes; // passes in the current schedule
+  return B200FFT_SUCCESS;
 }
 
 } // extern "C"

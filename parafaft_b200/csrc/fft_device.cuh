@@ -186,6 +186,43 @@ BF_D void apply_twiddles(V *v, const V *tw, int base) {
   }
 }
 
+// Same with a twiddle pyramid: tn points at T_n[k] = exp(-2*pi*i*k/n) and the
+// tables T_{n/2}, T_{n/4} follow it (offsets n and 3n/2), so w = T_n[k],
+// w^2 = T_{n/2}[k] and w^4 = T_{n/4}[k] are loads that are contiguous across
+// neighbouring k.
+template <int R, bool CONJ, typename V>
+BF_D void apply_twiddles_pyr(V *v, const V *tn, int n, int k) {
+  if constexpr (R == 2) {
+    v[1] = cmulw<CONJ>(v[1], ldtw(tn, k));
+  } else if constexpr (R == 4) {
+    const V w1 = ldtw(tn, k), w2 = ldtw(tn, n + k);
+    v[1] = cmulw<CONJ>(v[1], w1);
+    v[2] = cmulw<CONJ>(v[2], w2);
+    v[3] = cmulw<CONJ>(v[3], cmulw<false>(w1, w2));
+  } else if constexpr (R == 8) {
+    const V w1 = ldtw(tn, k), w2 = ldtw(tn, n + k), w4 = ldtw(tn, n + n / 2 + k);
+    const V w3 = cmulw<false>(w1, w2);
+    v[1] = cmulw<CONJ>(v[1], w1);
+    v[2] = cmulw<CONJ>(v[2], w2);
+    v[3] = cmulw<CONJ>(v[3], w3);
+    v[4] = cmulw<CONJ>(v[4], w4);
+    v[5] = cmulw<CONJ>(v[5], cmulw<false>(w4, w1));
+    v[6] = cmulw<CONJ>(v[6], cmulw<false>(w4, w2));
+    v[7] = cmulw<CONJ>(v[7], cmulw<false>(w4, w3));
+  } else {
+#pragma unroll
+    for (int r = 1; r < R; ++r)
+      v[r] = cmulw<CONJ>(v[r], ldtw(tn, (r * k) % n));
+  }
+}
+
+template <typename V> BF_D V shfl_cplx(V x, int src, int width) {
+  V r;
+  r.x = __shfl_sync(0xffffffffu, x.x, src, width);
+  r.y = __shfl_sync(0xffffffffu, x.y, src, width);
+  return r;
+}
+
 // ==========================================================================
 // Family S: lengths known at compile time (powers of two up to 4096).
 // ==========================================================================
@@ -217,6 +254,21 @@ struct KS {
     return e;
   }
   static constexpr int EMAX = emax();
+
+  static constexpr bool all_full() {
+    for (int s = 0; s < S.nst; ++s)
+      if ((L / S.rad[s]) % P != 0)
+        return false;
+    return true;
+  }
+  // Row transforms held by P <= 32 lanes of one warp, every stage evenly
+  // split: lane g owns points g + P*m, m < L/P, in the first stage's inputs
+  // and the last stage's outputs. The Hermitian partner L - k of point
+  // k = g + P*m then sits in lane P - g at m' = L/P - 1 - m (lane 0: its own
+  // point P*(L/P - m)), so R2C/C2R pair points with warp shuffles instead of
+  // a pass through shared memory.
+  static constexpr bool SHUF = !COL && KIND != KIND_C2C && P <= 32 && all_full();
+  static constexpr int TM = L * TSCALE; // top length of the twiddle pyramid
 
   static constexpr size_t smem_bytes() {
     return static_cast<size_t>(TB) * LP * sizeof(V) * (STAGED ? 2 : 1);
@@ -259,6 +311,24 @@ struct KS {
     return cmake(e.x - o.y, e.y + o.x);
   }
 
+  // R2C output X[k] from za = Z[k], zb = Z[L-k], w = exp(-2*pi*i*k/(2L)):
+  // X = E + w*O, E = (za + conj zb)/2, O = -i (za - conj zb)/2.
+  static BF_D V r2c_from_pair(V za, V zb, V w) {
+    const V b = cconj(zb);
+    const V e = cmake(T(0.5) * (za.x + b.x), T(0.5) * (za.y + b.y));
+    const V d = csub(za, b);
+    const V o = cmake(T(0.5) * d.y, T(-0.5) * d.x);
+    return cadd(e, cmulw<false>(o, w));
+  }
+
+  // C2R input Z[n] from xa = X[n], xb = X[L-n], w = exp(-2*pi*i*n/(2L)):
+  // Z = E + i*O, E = xa + conj xb, O = (xa - conj xb) * conj(w).
+  static BF_D V c2r_from_pair(V xa, V xb, V w) {
+    const V e = cadd(xa, cconj(xb));
+    const V o = cmulw<true>(csub(xa, cconj(xb)), w);
+    return cmake(e.x - o.y, e.y + o.x);
+  }
+
   // R2C output k in [0, L] from Z held in shared memory (natural order).
   // w = exp(-2*pi*i*k/(2L)).
   static BF_D V r2c_post(const Ctx &c, int k, V w) {
@@ -282,7 +352,7 @@ struct KS {
         const int j = c.g + P * i;
         if (FULL || j < B) {
           const int k = j % Ns;
-          apply_twiddles<R, !FWD>(&v[i * R], c.tw, k * (L / (Ns * R)) * TSCALE);
+          apply_twiddles_pyr<R, !FWD>(&v[i * R], c.tw + (2 * TM - 2 * Ns * R), Ns * R, k);
         }
       }
     }
@@ -291,7 +361,28 @@ struct KS {
       dft<R, FWD>(&v[i * R]);
 
     if constexpr (s == NST - 1) {
-      if constexpr (KIND == KIND_R2C) {
+      if constexpr (KIND == KIND_R2C && SHUF) {
+        // lane g holds Z[g + P*m] in v[(m % BP)*R + m / BP]
+        constexpr int NM = L / P;
+        constexpr int BP = B / P;
+        const V wg = ldtw(c.tw, c.g);
+        const int src = (P - c.g) & (P - 1);
+#pragma unroll
+        for (int m = 0; m < NM; ++m) {
+          const int mp = NM - 1 - m;
+          V zb = shfl_cplx(v[(mp % BP) * R + mp / BP], src, P);
+          if (c.g == 0) {
+            const int m2 = (NM - m) % NM;
+            zb = v[(m2 % BP) * R + m2 / BP];
+          }
+          const V za = v[(m % BP) * R + m / BP];
+          const V w = m == 0 ? wg : cmulw<false>(wg, ldtw(c.tw, P * m));
+          if (c.act)
+            c.gout[(long long)(c.g + P * m) * c.ost] = r2c_from_pair(za, zb, w);
+        }
+        if (c.act && c.g == 0) // X[L] = Re Z[0] - Im Z[0]
+          c.gout[(long long)L * c.ost] = cmake(v[0].x - v[0].y, T(0));
+      } else if constexpr (KIND == KIND_R2C) {
         if constexpr (s > 0)
           bar();
 #pragma unroll
@@ -385,6 +476,35 @@ struct KS {
     constexpr int B = L / R;
     constexpr int K = (B + P - 1) / P;
     constexpr bool FULL = (B % P) == 0;
+    if constexpr (KIND == KIND_C2R && SHUF) {
+      // lane g loads X[g + P*m] (coalesced) and lane 0 also X[L]; the
+      // partner X[L - n] comes from lane P - g by shuffle.
+      constexpr int NM = L / P;
+      constexpr int BP = B / P;
+      V x[NM];
+#pragma unroll
+      for (int m = 0; m < NM; ++m)
+        x[m] = c.act ? c.gin[(long long)(c.g + P * m) * c.ist] : czero<V>();
+      const V xl = (c.act && c.g == 0) ? c.gin[(long long)L * c.ist] : czero<V>();
+      const V wg = ldtw(c.tw, c.g);
+      const int src = (P - c.g) & (P - 1);
+#pragma unroll
+      for (int m = 0; m < NM; ++m) {
+        V xb = shfl_cplx(x[NM - 1 - m], src, P);
+        V xa = x[m];
+        if (c.g == 0) {
+          xb = m == 0 ? xl : x[NM - m];
+          if (m == 0) { // Im of DC and Nyquist are ignored
+            xa.y = T(0);
+            xb.y = T(0);
+          }
+        }
+        const V w = m == 0 ? wg : cmulw<false>(wg, ldtw(c.tw, P * m));
+        v[(m % BP) * R + m / BP] = c2r_from_pair(xa, xb, w);
+      }
+      run<0>(c, v);
+      return;
+    }
 #pragma unroll
     for (int i = 0; i < K; ++i) {
       const int j = c.g + P * i;
@@ -484,8 +604,14 @@ struct KS {
   }
 };
 
+// 256-thread column kernels keep two CTAs per SM (at most 128 registers):
+// left alone, the compiler hoists the twiddle loads of later stages and
+// drops to one CTA per SM, which halves the loads in flight.
+#ifndef B2_COL_MIN_BLOCKS
+#define B2_COL_MIN_BLOCKS 2
+#endif
 template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, (COL && NT == 256) ? B2_COL_MIN_BLOCKS : 1)
     fft_static_kernel(const PassArgs a) {
   using K = KS<T, L, NT, TB, COL, FWD, KIND>;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -552,16 +678,17 @@ BF_D void gen_butterfly_prime(const GenArgs &a, const V *A, V *Bm, const V *tw,
   }
 }
 
+// One tile (a.TB transforms) of a generic pass, run by a whole CTA of
+// kGenThreads threads with 2*TB*L elements of dynamic shared memory.
 template <typename T, bool COL, int KIND, bool FWD>
-__global__ void __launch_bounds__(kGenThreads) fft_generic_kernel(const GenArgs a) {
+BF_D void gen_tile(const GenArgs &a, long long tile, unsigned char *smraw) {
   using V = cvec<T>;
-  extern __shared__ __align__(16) unsigned char smraw[];
   V *A = reinterpret_cast<V *>(smraw);
   V *Bm = A + static_cast<size_t>(a.TB) * a.L;
   const V *tw = reinterpret_cast<const V *>(a.p.tw);
   const int tid = threadIdx.x;
   const int TB = a.TB, L = a.L;
-  const long long tile0 = static_cast<long long>(blockIdx.x) * TB;
+  const long long tile0 = tile * TB;
 
   auto offsets = [&](int tb, long long &io, long long &oo) -> bool {
     const long long b = tile0 + tb;
@@ -697,6 +824,52 @@ __global__ void __launch_bounds__(kGenThreads) fft_generic_kernel(const GenArgs 
         x[(2LL * k + 1) * os] = z.y;
       }
     }
+  }
+}
+
+template <typename T, bool COL, int KIND, bool FWD>
+__global__ void __launch_bounds__(kGenThreads) fft_generic_kernel(const GenArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  gen_tile<T, COL, KIND, FWD>(a, blockIdx.x, smraw);
+}
+
+// Persistent grouped pass: CTAs take tiles from a device work queue (one
+// atomic counter) until all tiles of all items are done. Item i covers tiles
+// [tile_start[i], tile_start[i+1]); items are passes of independent
+// transforms (for example the same stage of many separate grids), each with
+// its own length, layout, pointers and twiddle table.
+template <typename T, bool COL, int KIND, bool FWD>
+__global__ void __launch_bounds__(kGenThreads)
+    fft_generic_group_kernel(const GenArgs *__restrict__ items,
+                             const long long *__restrict__ tile_start, int nitems,
+                             unsigned long long *queue) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ long long task_s;
+  __shared__ int item_s;
+  const long long ntasks = tile_start[nitems];
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long long t = static_cast<long long>(atomicAdd(queue, 1ull));
+      int lo = 0, hi = nitems - 1;
+      if (t < ntasks) {
+        while (lo < hi) { // last item whose first tile is <= t
+          const int mid = (lo + hi + 1) >> 1;
+          if (tile_start[mid] <= t)
+            lo = mid;
+          else
+            hi = mid - 1;
+        }
+      }
+      task_s = t;
+      item_s = lo;
+    }
+    __syncthreads();
+    const long long t = task_s;
+    const int i = item_s;
+    if (t >= ntasks)
+      return;
+    gen_tile<T, COL, KIND, FWD>(items[i], t - tile_start[i], smraw);
+    __syncthreads(); // shared memory and task_s are reused by the next tile
   }
 }
 

@@ -8,15 +8,18 @@
 namespace b200fft {
 
 // ==========================================================================
-// Twiddle table exp(-2*pi*i*m/n), m in [0, n), computed in FP64.
-// 4m = q*n + r with integers q (quadrant) and r < n; the angle is
-// (pi/2)(q + r/n); the remainder is folded to [0, n/2] so sincospi gets an
-// argument in [0, 1/4] that carries no reduction error.
+// Twiddle tables, computed in FP64 and rounded once.
+// exp(-2*pi*i*m/n): 4m = q*n + r with integers q (quadrant) and r < n; the
+// angle is (pi/2)(q + r/n); the remainder is folded to [0, n/2] so sincospi
+// gets an argument in [0, 1/4] that carries no reduction error.
+//
+// For a power-of-two top length M the table is a pyramid: the M-point table
+// T_M[k] = exp(-2*pi*i*k/M), then T_{M/2}, T_{M/4}, ..., T_1, with T_n at
+// offset 2M - 2n (2M - 1 entries). T_M alone (offset 0) is what the generic
+// kernels index; the specialised kernels read stage twiddles w^p for
+// w = exp(-2*pi*i/n) as T_{n/p}[k], contiguous in k. Other lengths get T_M only.
 // ==========================================================================
-__global__ void twiddle_table_kernel(double2 *t64, float2 *t32, int n) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= n)
-    return;
+__device__ double2 twiddle_fp64(long long m, long long n) {
   const long long t = 4LL * m;
   const int q = static_cast<int>(t / n);
   const long long r = t - static_cast<long long>(q) * n;
@@ -36,13 +39,24 @@ __global__ void twiddle_table_kernel(double2 *t64, float2 *t32, int n) {
   case 2: cr = -c; ci = -s; break;
   default: cr = s; ci = -c; break;
   }
-  const double2 w = make_double2(cr, -ci);
-  if (t64)
-    t64[m] = w;
-  if (t32)
-    t32[m] = make_float2(static_cast<float>(w.x), static_cast<float>(w.y));
+  return make_double2(cr, -ci);
 }
 
+__global__ void twiddle_table_kernel(double2 *t64, float2 *t32, int M, int entries) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= entries)
+    return;
+  long long n = M, off = 0;
+  while (i >= off + n) { // pyramid level of entry i (only for power-of-two M)
+    off += n;
+    n >>= 1;
+  }
+  const double2 w = twiddle_fp64(i - off, n);
+  if (t64)
+    t64[i] = w;
+  if (t32)
+    t32[i] = make_float2(static_cast<float>(w.x), static_cast<float>(w.y));
+}
 
 namespace {
 
@@ -92,6 +106,52 @@ cudaError_t launch_g_t(int kind, bool col, bool fwd, const GenArgs &g,
 
 } // namespace
 
+namespace {
+template <typename T, bool COL, int KIND, bool FWD>
+cudaError_t launch_gg(const GenArgs *items, const long long *tile_start, int nitems,
+                      unsigned long long *queue, size_t smem, int grid, cudaStream_t st) {
+  auto kern = fft_generic_group_kernel<T, COL, KIND, FWD>;
+  if (smem > kGenericSmemLimit)
+    return cudaErrorInvalidValue;
+  // the kernel also holds a few bytes of static shared memory, so opt in
+  // above 48 KiB of total, not of dynamic, shared memory
+  if (smem + 256 > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kGenericSmemLimit));
+    if (e != cudaSuccess)
+      return e;
+  }
+  kern<<<grid, kGenThreads, smem, st>>>(items, tile_start, nitems, queue);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_gg_t(int kind, bool col, bool fwd, const GenArgs *items,
+                        const long long *tile_start, int nitems, unsigned long long *queue,
+                        size_t smem, int grid, cudaStream_t st) {
+  if (kind == KIND_C2C) {
+    if (col)
+      return fwd ? launch_gg<T, true, KIND_C2C, true>(items, tile_start, nitems, queue, smem, grid, st)
+                 : launch_gg<T, true, KIND_C2C, false>(items, tile_start, nitems, queue, smem, grid, st);
+    return fwd ? launch_gg<T, false, KIND_C2C, true>(items, tile_start, nitems, queue, smem, grid, st)
+               : launch_gg<T, false, KIND_C2C, false>(items, tile_start, nitems, queue, smem, grid, st);
+  }
+  if (kind == KIND_R2C)
+    return col ? launch_gg<T, true, KIND_R2C, true>(items, tile_start, nitems, queue, smem, grid, st)
+               : launch_gg<T, false, KIND_R2C, true>(items, tile_start, nitems, queue, smem, grid, st);
+  return col ? launch_gg<T, true, KIND_C2R, false>(items, tile_start, nitems, queue, smem, grid, st)
+             : launch_gg<T, false, KIND_C2R, false>(items, tile_start, nitems, queue, smem, grid, st);
+}
+} // namespace
+
+cudaError_t launch_generic_group(bool f64, int kind, bool col, bool fwd, const GenArgs *items,
+                                 const long long *tile_start, int nitems,
+                                 unsigned long long *queue, size_t smem, int grid,
+                                 cudaStream_t st) {
+  return f64 ? launch_gg_t<double>(kind, col, fwd, items, tile_start, nitems, queue, smem, grid, st)
+             : launch_gg_t<float>(kind, col, fwd, items, tile_start, nitems, queue, smem, grid, st);
+}
+
 cudaError_t launch_generic(bool f64, int kind, bool col, bool fwd,
                            const GenArgs &g, cudaStream_t st) {
   return f64 ? launch_g_t<double>(kind, col, fwd, g, st)
@@ -108,13 +168,16 @@ size_t static_smem_bytes(int esize_complex, int L, bool col, int var) {
   return esize_complex == 16 ? smem_s<double>(L, col, var) : smem_s<float>(L, col, var);
 }
 
+int twiddle_table_entries(int n) { return is_pow2(n) ? 2 * n - 1 : n; }
+
 cudaError_t launch_twiddle_table(double2 *t64, float2 *t32, int n,
                                  cudaStream_t st) {
   if (n <= 0)
     return cudaErrorInvalidValue;
+  const int entries = twiddle_table_entries(n);
   const int threads = 256;
-  const int blocks = (n + threads - 1) / threads;
-  twiddle_table_kernel<<<blocks, threads, 0, st>>>(t64, t32, n);
+  const int blocks = (entries + threads - 1) / threads;
+  twiddle_table_kernel<<<blocks, threads, 0, st>>>(t64, t32, n, entries);
   return cudaGetLastError();
 }
 

@@ -27,9 +27,18 @@ size_t static_smem_bytes(int esize_complex, int L, bool col, int var);
 cudaError_t launch_generic(bool f64, int kind, bool col, bool fwd,
                            const GenArgs &g, cudaStream_t st);
 size_t generic_smem_bytes(bool f64, int TB, int L);
+// Persistent grouped generic pass over device arrays of items (device
+// pointers): CTAs take tiles from *queue (zeroed before the launch).
+cudaError_t launch_generic_group(bool f64, int kind, bool col, bool fwd, const GenArgs *items,
+                                 const long long *tile_start, int nitems,
+                                 unsigned long long *queue, size_t smem, int grid,
+                                 cudaStream_t st);
 constexpr size_t kGenericSmemLimit = 200 * 1024;
 
-// FP64 twiddle table exp(-2*pi*i*m/n) (t64 and/or t32 may be null).
+// Entries of the twiddle table of top length n: a pyramid T_n, T_{n/2}, ...,
+// T_1 for powers of two (2n - 1 entries), else T_n alone.
+int twiddle_table_entries(int n);
+// FP64-computed twiddle table of top length n (t64 and/or t32 may be null).
 cudaError_t launch_twiddle_table(double2 *t64, float2 *t32, int n,
                                  cudaStream_t st);
 

@@ -10,7 +10,7 @@
 //
 // How: the one piece of memory the transform needs besides its input and
 // output, the twiddle table, lives in a fixed array in the library's own
-// device image (4096 complex doubles, 64 KiB, held on every device that loads
+// device image (8192 complex doubles, 128 KiB, held on every device that loads
 // the library until the process exits). Each call rewrites the table for its
 // length in that array and then runs the specialised C2C kernel on the
 // caller's stream; nothing in the array has to start at zero.
@@ -40,11 +40,12 @@ void set_error_text(const std::string &msg); // api.cu: text of b200fft_last_err
 
 #define NOALLOC_MAX_LENGTH 4096
 
-// The twiddle table of b200fft_c2c_noalloc: NOALLOC_MAX_LENGTH complex doubles
-// (64 KiB). Host code must not pass this name to a kernel: on the host it only
-// stands for the symbol. The device address comes from cudaGetSymbolAddress
-// (device_table below).
-static __device__ __align__(256) unsigned char g_noalloc_table[NOALLOC_MAX_LENGTH * 16];
+// The twiddle table of b200fft_c2c_noalloc: 2 * NOALLOC_MAX_LENGTH complex
+// doubles (128 KiB), room for the table pyramid of the longest length. Host
+// code must not pass this name to a kernel: on the host it only stands for the
+// symbol. The device address comes from cudaGetSymbolAddress (device_table
+// below).
+static __device__ __align__(256) unsigned char g_noalloc_table[2 * NOALLOC_MAX_LENGTH * 16];
 
 namespace {
 

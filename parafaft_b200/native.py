@@ -38,6 +38,9 @@ ENGINE_SYMBOLS = (
     "b200fft_sync", "b200fft_flush", "b200fft_alloc", "b200fft_free",
     "b200fft_get_stats", "b200fft_reset_stats", "b200fft_get_log", "b200fft_set_profiling",
     "b200fft_describe", "b200fft_supported", "b200fft_c2c_noalloc",
+    "b200fft_group_create", "b200fft_group_destroy", "b200fft_group_add",
+    "b200fft_group_begin", "b200fft_group_end", "b200fft_group_capture",
+    "b200fft_group_replay", "b200fft_group_sync", "b200fft_group_stats",
 )
 
 
@@ -106,6 +109,15 @@ def engine() -> C.CDLL:
             "b200fft_describe": (i, [i, i, i, sz, pd, pd, C.c_char_p, sz]),
             "b200fft_supported": (i, [i, i, i]),
             "b200fft_c2c_noalloc": (i, [i, i, i, sz, pd, pd, vp, vp, vp]),
+            "b200fft_group_create": (i, [C.POINTER(vp)]),
+            "b200fft_group_destroy": (i, [vp]),
+            "b200fft_group_add": (i, [vp, vp]),
+            "b200fft_group_begin": (i, [vp]),
+            "b200fft_group_end": (i, [vp]),
+            "b200fft_group_capture": (i, [vp]),
+            "b200fft_group_replay": (i, [vp]),
+            "b200fft_group_sync": (i, [vp]),
+            "b200fft_group_stats": (i, [vp, C.POINTER(Stats)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -246,6 +258,57 @@ class Handle:
         n = C.c_int()
         check(self._lib.b200fft_get_log(self._h, buf, cap, C.byref(n)))
         return [buf[i].as_dict() for i in range(n.value)]
+
+
+class Group:
+    """b200fft_group: transforms of many handles launched together."""
+
+    def __init__(self, handles=()):
+        self._lib = engine()
+        g = C.c_void_p()
+        check(self._lib.b200fft_group_create(C.byref(g)))
+        self._g = g
+        self.members = []
+        for h in handles:
+            self.add(h)
+
+    def add(self, h: "Handle"):
+        check(self._lib.b200fft_group_add(self._g, h.raw))
+        self.members.append(h)
+
+    def begin(self):
+        check(self._lib.b200fft_group_begin(self._g))
+
+    def end(self):
+        check(self._lib.b200fft_group_end(self._g))
+
+    def capture(self):
+        check(self._lib.b200fft_group_capture(self._g))
+
+    def replay(self):
+        check(self._lib.b200fft_group_replay(self._g))
+
+    def sync(self):
+        check(self._lib.b200fft_group_sync(self._g))
+
+    def stats(self) -> dict:
+        s = Stats()
+        check(self._lib.b200fft_group_stats(self._g, C.byref(s)))
+        d = s.as_dict()
+        d["passes_per_run"] = d.pop("coalesced_calls")
+        d["runs"] = d.pop("exec_calls")
+        return d
+
+    def close(self):
+        if self._g:
+            check(self._lib.b200fft_group_destroy(self._g))
+            self._g = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def describe(precision: int, kind: int, length: int, batch: int = 1, stride: int = 1,

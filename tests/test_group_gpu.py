@@ -1,0 +1,104 @@
+"""Batches of independent uneven grids through groups (the C3 path).
+
+Each grid is its own ParaFaFT_R2C<3, B200Backend<float>> object; their
+forward+backward passes are recorded in one group and launched together, then
+replayed, then replayed from a CUDA graph. Every run must equal the per-grid
+result and the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from helpers import REL_F32, to_dev, to_host
+from oracle import oracle as O
+from parafaft_b200 import native as nv
+
+pytestmark = pytest.mark.gpu
+
+SIDES = [32, 48, 60, 64, 80, 96, 120, 128, 160]
+
+
+def _drivers_or_skip():
+    try:
+        nv.drivers()
+    except ImportError as e:
+        pytest.skip(str(e))
+
+
+def _grids(n, seed):
+    rng = np.random.default_rng(seed)
+    return [tuple(int(x) for x in rng.choice(SIDES, 3)) for _ in range(n)]
+
+
+def test_group_forward_matches_oracle_and_per_grid():
+    _drivers_or_skip()
+    shapes = _grids(12, 5)
+    objs, devs, xs = [], [], []
+    for i, shp in enumerate(shapes):
+        x = O.gaussian_random_field(shp, 100 + i).astype(np.float32)
+        f = nv.ParaFaFT("r2c", shp, nv.F32)
+        buf = np.zeros(f.required_size, np.float32)
+        p = O.pad_real(x, np.float32)
+        buf[:p.size] = p
+        objs.append(f)
+        devs.append(to_dev(buf))
+        xs.append(x)
+    g = nv.Group([f.handle() for f in objs])
+    g.begin()
+    for f, d in zip(objs, devs):
+        f.forward(d)
+    g.end()
+    g.sync()
+    assert g.stats()["kernel_launches"] == 3
+    for shp, x, d in zip(shapes, xs, devs):
+        nc = shp[-1] // 2 + 1
+        X = to_host(d)[:2 * shp[0] * shp[1] * nc].view(np.complex64).reshape(shp[0], shp[1], nc)
+        assert O.rel_l2(X, O.r2c_nd(x.astype(np.float64))) < REL_F32, shp
+
+
+def test_group_roundtrip_replay_and_graph():
+    _drivers_or_skip()
+    shapes = _grids(20, 9)
+    objs, devs, xs = [], [], []
+    for i, shp in enumerate(shapes):
+        x = O.normal_real(shp, i).astype(np.float32)
+        f = nv.ParaFaFT("r2c", shp, nv.F32)
+        buf = np.zeros(f.required_size, np.float32)
+        p = O.pad_real(x, np.float32)
+        buf[:p.size] = p
+        objs.append(f)
+        devs.append(to_dev(buf))
+        xs.append(x)
+    g = nv.Group([f.handle() for f in objs])
+    g.begin()
+    for f, d in zip(objs, devs):
+        f.forward(d)
+        f.backward(d)
+    g.end()
+    g.sync()
+    scale = [float(np.prod(s)) for s in shapes]
+
+    def check(k):
+        for shp, x, d, sc in zip(shapes, xs, devs, scale):
+            y = O.unpad_real(to_host(d)[:O.pad_real(x).size], shp) / sc ** k
+            assert O.rel_l2(y, x) < 4 * REL_F32, (shp, k)
+
+    check(1)
+    # each run scales by N again (unnormalised forward+backward)
+    for d, sc in zip(devs, scale):
+        d.mul_(1.0 / sc)
+    g.replay()
+    g.sync()
+    check(1)
+    for d, sc in zip(devs, scale):
+        d.mul_(1.0 / sc)
+    g.capture()
+    g.replay()
+    g.sync()
+    check(1)
+    st = g.stats()
+    assert st["kernel_launches"] == 12 and st["passes_per_run"] == 20 * 6
+    g.close()
+    # members work on their own again after the group is gone
+    for f, d in zip(objs[:2], devs[:2]):
+        f.forward(d)
+        f.backward(d)

@@ -152,3 +152,30 @@ st = f.handle().stats()
 print(st["kernel_launches"], st["copies_issued"])
 ''')
     assert out.split() == ["34", "2"]
+
+
+@pytest.mark.skipif(not _drivers_built(), reason="ParaFaFT drivers not built")
+def test_group_schedules_many_grids_in_six_launches():
+    """256 ParaFaFT_R2C<3> objects of uneven sizes, forward+backward recorded in
+    one group: 6 grouped launches (one per pass depth), 256*6 passes, no copies."""
+    out = _run_record(r'''
+import ctypes as C, numpy as np
+from parafaft_b200 import native as nv
+rng = np.random.default_rng(3)
+sides = [32, 48, 60, 64, 80, 96, 120, 128, 160]
+objs, bufs = [], []
+for i in range(256):
+    shape = tuple(int(x) for x in rng.choice(sides, 3))
+    f = nv.ParaFaFT("r2c", shape, nv.F32)
+    b = C.c_void_p(); nv.check(nv.engine().b200fft_alloc(f.required_size * 4, C.byref(b)))
+    objs.append(f); bufs.append(b)
+g = nv.Group([f.handle() for f in objs])
+g.begin()
+for f, b in zip(objs, bufs):
+    f.forward(b.value)
+    f.backward(b.value)
+g.end()
+st = g.stats()
+print(st["kernel_launches"], st["passes_per_run"], st["copies_issued"])
+''')
+    assert out.split() == ["6", str(256 * 6), "0"]
