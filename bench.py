@@ -214,6 +214,124 @@ def run_kernels_only(args):
     return 0
 
 
+C2C_CONFIGS = {
+    # name: (shape, precision, orchestrator, input distribution, seed)
+    "c2c64": ((64, 64, 64), "f64", "c2c", "uniform", 11),
+    "c2c1024": ((1024, 1024, 1024), "f32", "c2c", "normal", 12),
+    "c2c4d": ((128, 128, 64, 64), "f64", "c2c_onerank", "uniform", 13),
+}
+
+
+def run_c2c_config(args):
+    """C2C forward+backward through ParaFaFT on B200Backend:
+      c2c64    64^3 complex128, ParaFaFT_C2C<3, B200Backend<double>>;
+      c2c1024  1024^3 complex64, ParaFaFT_C2C<3, B200Backend<float>>;
+      c2c4d    128x128x64x64 complex128 through the one-rank orchestrator (the
+               reference ParaFaFT_C2C mis-sizes non-hypercubic grids).
+    Accuracy: forward rel-L2 against an FP64 reference (the C oracle for 64^3,
+    scipy.fft FP64 for the 4D grid, the B200 FP64 path for 1024^3 whose
+    complex128 copy would not fit a host comparison) and the round trip."""
+    import torch
+    from parafaft_b200 import native as nv
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+    shape, prec_s, kind, dist, seed = C2C_CONFIGS[args.config]
+    prec = nv.F64 if prec_s == "f64" else nv.F32
+    ctype = torch.complex128 if prec == nv.F64 else torch.complex64
+    n = int(np.prod(shape))
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    if dist == "uniform":
+        re = torch.rand(n, generator=gen, device="cuda", dtype=torch.float64) * 2 - 1
+        im = torch.rand(n, generator=gen, device="cuda", dtype=torch.float64) * 2 - 1
+    else:
+        re = torch.randn(n, generator=gen, device="cuda", dtype=torch.float64)
+        im = torch.randn(n, generator=gen, device="cuda", dtype=torch.float64)
+    x64 = torch.complex(re, im)
+    del re, im
+    f = nv.ParaFaFT(kind, shape, prec)
+    assert f.required_size >= n
+    data = torch.zeros(f.required_size, dtype=ctype, device="cuda")
+    data[:n] = x64.to(ctype)
+    # ---- accuracy
+    f.forward(data)
+    y = data[:n].clone()
+    if args.config == "c2c64":
+        ref = torch.from_numpy(O.c2c_nd(x64.cpu().numpy().reshape(shape)).reshape(-1)).cuda()
+        ref_src = "C oracle FP64"
+    elif args.config == "c2c4d":
+        ref = torch.from_numpy(O.c2c_nd(x64.cpu().numpy().reshape(shape), -1, "scipy").reshape(-1)).cuda()
+        ref_src = "scipy.fft FP64"
+    else:
+        g64 = nv.ParaFaFT(kind, shape, nv.F64)
+        d64 = torch.zeros(g64.required_size, dtype=torch.complex128, device="cuda")
+        d64[:n] = x64
+        g64.forward(d64)
+        ref = d64[:n]
+        ref_src = "B200 FP64 path"
+    rel_fwd = float(torch.linalg.vector_norm(y.to(torch.complex128) - ref) /
+                    torch.linalg.vector_norm(ref))
+    del ref
+    if args.config == "c2c1024":
+        del d64, g64
+    f.backward(data)
+    rel_rt = float(torch.linalg.vector_norm(data[:n].to(torch.complex128) / n - x64) /
+                   torch.linalg.vector_norm(x64))
+    del y
+    # ---- timing
+    data[:n] = x64.to(ctype)
+    del x64
+    h = f.handle()
+    stream = torch.cuda.Stream()
+    h.set_stream(stream.cuda_stream)
+    for _ in range(args.warmup):
+        f.forward(data)
+        f.backward(data)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    h.reset_stats()
+    e0.record(stream)
+    for _ in range(args.steps):
+        f.forward(data)
+        f.backward(data)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    st = h.stats()
+    h.set_profiling(True)
+    h.reset_stats()
+    for _ in range(max(2, args.steps // 4)):
+        f.forward(data)
+        f.backward(data)
+    log = h.log()
+    h.set_profiling(False)
+    per = {}
+    for r in log:
+        if r["kind"] == 3:
+            continue
+        key = f"stage{r['stage']}_" + ("fwd" if r["direction"] == 0 else "bwd")
+        per.setdefault(key, []).append((r["ms"], r["bytes"]))
+    kernels = {k: {"ms": round(float(np.mean([m for m, _ in v])), 4),
+                   "GBps": round(v[0][1] / np.mean([m for m, _ in v]) / 1e6, 1)} for k, v in per.items()}
+    esz = 16 if prec == nv.F64 else 8
+    alg = 2 * len(shape) * 2 * n * esz
+    peak, peak_kind = _peaks()
+    line = {
+        "metric": f"{args.config} C2C fwd+bwd ms", "value": round(ms, 4), "unit": "ms",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+        "dtype": prec_s, "data": f"synthetic {dist} complex, seed {seed}",
+        "config": {"workload": f"{kind} {'x'.join(map(str, shape))} {prec_s}", "orchestrator": kind},
+        "rel_l2_fwd": rel_fwd, "rel_l2_reference": ref_src, "rel_l2_roundtrip": rel_rt,
+        "alg_bytes": alg, "hbm_frac": round(alg / (ms * 1e-3) / 1e9 / peak, 4),
+        "peak_source": peak_kind, "kernels": kernels,
+        "gpu_launches_per_step": st["kernel_launches"] / args.steps,
+        "copies_issued_per_step": st["copies_issued"] / args.steps,
+    }
+    print(json.dumps(line), flush=True)
+    f.close()
+    return 0
+
+
 UNEVEN_SIDES = [32, 48, 60, 64, 80, 96, 120, 128, 160]
 
 
@@ -507,8 +625,10 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=150.0)
     ap.add_argument("--kernels-only", action="store_true",
                     help="run only the timed loop (used for ncu captures)")
-    ap.add_argument("--config", default="r2c512", choices=["r2c512", "uneven256"],
-                    help="r2c512: the headline 512^3 R2C; uneven256: 256 uneven grids")
+    ap.add_argument("--config", default="r2c512",
+                    choices=["r2c512", "uneven256", "c2c64", "c2c1024", "c2c4d"],
+                    help="r2c512: the headline 512^3 R2C (default); uneven256: 256 "
+                         "uneven grids; c2c64 / c2c1024 / c2c4d: the C2C configurations")
     ap.add_argument("--grids", type=int, default=256)
     ap.add_argument("--seed", type=int, default=2024)
     args = ap.parse_args()
@@ -520,6 +640,8 @@ def main():
         return run_kernels_only(args)
     if args.config == "uneven256":
         return run_uneven(args)
+    if args.config in C2C_CONFIGS:
+        return run_c2c_config(args)
     return run_b200(args)
 
 

@@ -148,6 +148,23 @@ int b200fft_sync(b200fft_handle h);
 /* Issue held-back work without blocking. */
 int b200fft_flush(b200fft_handle h);
 
+/* ---- planning with measurement (FFTPlanFlag::Measure / Patient) ---------- */
+/* Buffer the next plans may use to time kernel candidates in place (contents
+ * are overwritten, as FFTW_MEASURE overwrites its planning array). ParaFaFT
+ * passes its scratch buffer to create_*_plan for this (parafaft_c2c.hpp:263-284,
+ * parafaft_r2c.hpp:1174-1203); B200Backend forwards it here. bytes = 0 means
+ * "large enough for every plan's layout". */
+int b200fft_set_work_buffer(b200fft_handle h, void *work, size_t bytes);
+/* The kernel a plan uses (kind 0 c2c with `stage`, 1 r2c, 2 c2r). */
+int b200fft_plan_describe(b200fft_handle h, int kind, int stage, char *buf,
+                          size_t buflen);
+/* Plan cache, the analogue of FFTW wisdom (fft_backend_fftw.hpp:666-694):
+ * measured choices keyed by GPU model and plan geometry. Import returns the
+ * number of entries read (or a negative status). */
+int b200fft_export_wisdom(const char *path);
+int b200fft_import_wisdom(const char *path);
+int b200fft_forget_wisdom(void);
+
 /* ---- device memory for the backend's Buffer/ComplexBuffer types
  *      (replaces cuvector<T>, fft_backend_cufft.hpp:58-121) --------------- */
 int b200fft_alloc(size_t bytes, void **ptr);

@@ -170,9 +170,12 @@ public:
   }
 
   // ---- C2C (fft_backend_cufft.hpp:292-337) --------------------------------
+  // With FFTPlanFlag::Measure/Patient the planning pointer (ParaFaFT's
+  // scratch buffer) is where kernel candidates are timed; its contents are
+  // overwritten, as with FFTW_MEASURE.
   void create_stage_plan(int stage, int length, std::size_t batch, Complex *data,
                          std::ptrdiff_t stride, std::ptrdiff_t dist) {
-    (void)data;
+    planning_buffer(data);
     b200_detail::check(b200fft_plan_c2c(h_, stage, length, batch, stride, dist),
                        "create_stage_plan");
   }
@@ -189,7 +192,7 @@ public:
   // ---- in-place R2C / C2R (fft_backend_cufft.hpp:360-469) -----------------
   void create_r2c_inplace_plan(int length, std::size_t batch, FloatType *padded_real,
                                std::ptrdiff_t stride, std::ptrdiff_t dist) {
-    (void)padded_real;
+    planning_buffer(padded_real);
     b200_detail::check(b200fft_plan_r2c(h_, length, batch, stride, dist),
                        "create_r2c_inplace_plan");
   }
@@ -198,7 +201,7 @@ public:
   }
   void create_c2r_inplace_plan(int length, std::size_t batch, FloatType *padded_real,
                                std::ptrdiff_t stride, std::ptrdiff_t dist) {
-    (void)padded_real;
+    planning_buffer(padded_real);
     b200_detail::check(b200fft_plan_c2r(h_, length, batch, stride, dist),
                        "create_c2r_inplace_plan");
   }
@@ -228,6 +231,11 @@ public:
   }
 
 private:
+  void planning_buffer(void *p) {
+    if (plan_flag_ != FFTPlanFlag::Estimate)
+      b200_detail::check(b200fft_set_work_buffer(h_, p, 0), "planning buffer");
+  }
+
   void open() {
     const int prec = std::is_same<FloatType, double>::value ? B200FFT_F64 : B200FFT_F32;
     const int pf = plan_flag_ == FFTPlanFlag::Estimate

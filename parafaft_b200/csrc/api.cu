@@ -158,9 +158,10 @@ int default_variant(int csize, int L, bool col, long long stride) {
   return 0;
 }
 
-// Choose the kernel for a plan. kind: KIND_C2C/R2C/C2R.
+// Choose the kernel for a plan. kind: KIND_C2C/R2C/C2R. `variant` >= 0 asks
+// for that tile-shape candidate of the specialised kernel (else the default).
 int choose_kernel(int prec, int kind, int len, long long batch, long long stride,
-                  long long dist, bool force_generic, Choice *out) {
+                  long long dist, bool force_generic, Choice *out, int variant = -1) {
   const int csize = prec == B200FFT_F64 ? 16 : 8;
   Choice ch;
   int L = len;
@@ -183,6 +184,8 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
     if (const char *v = std::getenv("B200FFT_VARIANT"))
       if (v[0] >= '0' && v[0] < '0' + kStaticVariants && v[1] == '\0')
         var = v[0] - '0';
+    if (variant >= 0 && variant < kStaticVariants)
+      var = variant;
     const CfgS c = cfg_static(csize, L, ch.col, var);
     ch.variant = var;
     ch.family = 0;
@@ -299,6 +302,9 @@ struct b200fft_handle_s {
   std::vector<cudaEvent_t> event_pool;
   size_t seq = 0;        // sequence number of the next log record
   size_t log_base = 0;   // sequence number of log.front()
+  // planning buffer for timing candidates (Measure/Patient plans)
+  void *work = nullptr;
+  size_t work_bytes = 0;
   // group membership (b200fft_group_*)
   b200fft_group_s *group = nullptr;
   bool recording = false;
@@ -539,6 +545,8 @@ int finish_fused_copy(H *h, const char *out0, size_t covered) {
 
 // Launch one pass of plan p. `in`/`out` point at the first transform;
 // slabs/slab (complex elements) describe a coalesced middle-axis run.
+cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a);
+
 // Kernel arguments of one pass of plan p run by kernel family `family`
 // (element units differ between the specialised and generic R2C/C2R kernels).
 PassArgs pass_args(const Plan &p, int family, const void *in, void *out, const void *tw,
@@ -615,7 +623,16 @@ int launch_pass(H *h, const Plan &p, int dir, const void *in, void *out,
     return B200FFT_SUCCESS;
   }
   ProfileScope ps(h);
+  const cudaError_t e = launch_kernel(h, p, dir, a);
+  push_log(h, r);
+  ps.done();
+  if (e != cudaSuccess)
+    return cuda_fail(e, "transform kernel launch");
+  return B200FFT_SUCCESS;
+}
 
+// The kernel launch of one pass (no bookkeeping).
+cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
   const bool f64 = h->prec == B200FFT_F64;
   const bool fwd = dir == B200FFT_FORWARD;
   cudaError_t e;
@@ -634,11 +651,7 @@ int launch_pass(H *h, const Plan &p, int dir, const void *in, void *out,
     g.p = a;
     e = launch_generic(f64, p.kind, p.ch.col, fwd, g, h->stream);
   }
-  push_log(h, r);
-  ps.done();
-  if (e != cudaSuccess)
-    return cuda_fail(e, "transform kernel launch");
-  return B200FFT_SUCCESS;
+  return e;
 }
 
 int flush_run(H *h) {
@@ -683,6 +696,154 @@ bool is_device_ptr(const void *p) {
   return at.type == cudaMemoryTypeDevice;
 }
 
+// ---- plan cache ("wisdom") and autotuner ------------------------------------
+// A wisdom entry records, for one plan geometry on one GPU model, the kernel
+// candidate that measured fastest and the planning rigor it was measured at
+// (1 Measure, 2 Patient). Planning at any rigor reuses an entry measured at
+// that rigor or above; b200fft_export_wisdom / b200fft_import_wisdom save and
+// load entries as text lines, like FFTW wisdom (fft_backend_fftw.hpp:666-694).
+struct WisdomVal {
+  int family = 0, variant = 0, rigor = 0;
+  double ms = 0.0;
+};
+std::mutex g_wis_mu;
+std::map<std::string, WisdomVal> g_wisdom;
+
+std::string device_tag(const H *h) {
+  if (h->record_only)
+    return "record-only";
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess) {
+    cudaGetLastError();
+    return "unknown";
+  }
+  std::string n = prop.name;
+  for (char &c : n)
+    if (c == ' ')
+      c = '_';
+  return n + "_sm" + std::to_string(prop.multiProcessorCount);
+}
+
+std::string wisdom_key(const H *h, const Plan &p, long long lead) {
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "%s p%d k%d n%d b%lld s%lld d%lld l%lld",
+                device_tag(h).c_str(), h->prec, p.kind, p.len, p.batch, p.stride, p.dist,
+                lead);
+  return buf;
+}
+
+size_t plan_region_bytes(const H *h, const Plan &p, long long lead) {
+  if (p.kind == KIND_C2C)
+    return lead > 1 ? static_cast<size_t>(lead) * p.len * p.batch * h->csize()
+                    : c2c_span_bytes(h, p);
+  return real_span_bytes(h, p);
+}
+
+// Time one candidate: 1 warm-up launch, then the mean of 3, in place on `work`.
+int time_candidate(H *h, const Plan &q, long long lead, double *ms) {
+  const void *tw = nullptr;
+  B2_TRY(get_table(h, q.ch.tlen, &tw));
+  const long long slab = lead > 1 ? static_cast<long long>(q.len) * q.batch : 0;
+  const PassArgs a = pass_args(q, q.ch.family, h->work, h->work, tw, lead, slab);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaError_t e = launch_kernel(h, q, B200FFT_FORWARD, a);
+  if (e == cudaSuccess)
+    e = cudaEventRecord(e0, h->stream);
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i)
+    e = launch_kernel(h, q, i % 2 ? B200FFT_BACKWARD : B200FFT_FORWARD, a);
+  if (e == cudaSuccess)
+    e = cudaEventRecord(e1, h->stream);
+  if (e == cudaSuccess)
+    e = cudaEventSynchronize(e1);
+  float t = 0.f;
+  if (e == cudaSuccess)
+    e = cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) {
+    // a candidate that cannot launch here is skipped, not fatal
+    cudaGetLastError();
+    *ms = -1.0;
+    return B200FFT_SUCCESS;
+  }
+  *ms = t / 3.0;
+  return B200FFT_SUCCESS;
+}
+
+// Pick the kernel of plan p by timing candidates (Measure: the default and
+// its closest alternatives; Patient: every tile shape and the generic
+// kernel), unless wisdom already has an answer of sufficient rigor.
+int autotune(H *h, Plan &p) {
+  const int rigor = h->plan_flag; // 1 Measure, 2 Patient
+  const long long lead = infer_lead(h, p);
+  const std::string key = wisdom_key(h, p, lead);
+  {
+    std::lock_guard<std::mutex> lk(g_wis_mu);
+    auto it = g_wisdom.find(key);
+    if (it != g_wisdom.end() && it->second.rigor >= rigor) {
+      Choice c;
+      if (choose_kernel(h->prec, p.kind, p.len, p.batch, p.stride, p.dist,
+                        it->second.family == 1, &c, it->second.variant) == B200FFT_SUCCESS) {
+        p.ch = c;
+        return B200FFT_SUCCESS;
+      }
+    }
+  }
+  if (h->record_only || h->work == nullptr)
+    return B200FFT_SUCCESS; // nothing to time on: keep the default
+  const size_t need = plan_region_bytes(h, p, lead);
+  if (h->work_bytes != 0 && need > h->work_bytes)
+    return B200FFT_SUCCESS;
+  std::vector<std::pair<int, int>> cands; // (family, variant)
+  if (p.ch.family == 0) {
+    if (p.ch.col) {
+      const int meas[] = {0, 3, 1};
+      const int pat[] = {0, 1, 2, 3, 4, 5};
+      if (rigor >= B200FFT_PLAN_PATIENT)
+        for (int v : pat) cands.push_back({0, v});
+      else
+        for (int v : meas) cands.push_back({0, v});
+    } else {
+      const int nv = rigor >= B200FFT_PLAN_PATIENT ? 3 : 2;
+      for (int v = 0; v < nv; ++v)
+        cands.push_back({0, v});
+    }
+  }
+  if (rigor >= B200FFT_PLAN_PATIENT || p.ch.family == 1)
+    cands.push_back({1, 0});
+  double best = -1.0;
+  Choice best_c = p.ch;
+  WisdomVal wv;
+  for (auto fv : cands) {
+    Choice c;
+    if (choose_kernel(h->prec, p.kind, p.len, p.batch, p.stride, p.dist, fv.first == 1, &c,
+                      fv.second) != B200FFT_SUCCESS)
+      continue;
+    if (c.family != fv.first)
+      continue;
+    Plan q = p;
+    q.ch = c;
+    double ms = -1.0;
+    B2_TRY(time_candidate(h, q, lead, &ms));
+    if (ms > 0 && (best < 0 || ms < best)) {
+      best = ms;
+      best_c = c;
+      wv.family = c.family;
+      wv.variant = c.variant;
+      wv.rigor = rigor;
+      wv.ms = ms;
+    }
+  }
+  if (best > 0) {
+    p.ch = best_c;
+    std::lock_guard<std::mutex> lk(g_wis_mu);
+    g_wisdom[key] = wv;
+  }
+  return B200FFT_SUCCESS;
+}
+
 int make_plan(H *h, Plan *dst, int kind, int length, size_t batch,
               ptrdiff_t stride, ptrdiff_t dist) {
   if (length < 1)
@@ -709,7 +870,12 @@ int make_plan(H *h, Plan *dst, int kind, int length, size_t batch,
   const void *tw = nullptr;
   B2_TRY(get_table(h, p.ch.tlen, &tw));
   p.valid = true;
-  *dst = p;
+  *dst = p; // visible to infer_lead while tuning
+  if (h->plan_flag >= B200FFT_PLAN_MEASURE && !h->force_generic &&
+      std::getenv("B200FFT_VARIANT") == nullptr) {
+    B2_TRY(autotune(h, p));
+    *dst = p;
+  }
   return B200FFT_SUCCESS;
 }
 
@@ -783,6 +949,12 @@ int b200fft_create(int precision, int num_stages, int plan_flag, unsigned flags,
     flags |= B200FFT_FLAG_NO_DEFER;
   if (env_flag("B200FFT_GENERIC_ONLY"))
     flags |= B200FFT_FLAG_GENERIC_ONLY;
+  static std::once_flag wisdom_once; // B200FFT_WISDOM=path: import once per process
+  std::call_once(wisdom_once, [] {
+    if (const char *w = std::getenv("B200FFT_WISDOM"))
+      if (w[0] != '\0')
+        b200fft_import_wisdom(w);
+  });
   H *h = new H();
   h->prec = precision;
   h->rsize = precision == B200FFT_F64 ? 8 : 4;
@@ -1041,6 +1213,97 @@ int b200fft_set_profiling(b200fft_handle h, int on) {
   B2_TRY(check_handle(h));
   B2_TRY(flush_all(h));
   h->profiling = on != 0;
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_set_work_buffer(b200fft_handle h, void *work, size_t bytes) {
+  B2_TRY(check_handle(h));
+  h->work = work;
+  h->work_bytes = bytes;
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_plan_describe(b200fft_handle h, int kind, int stage, char *buf, size_t buflen) {
+  B2_TRY(check_handle(h));
+  if (buf == nullptr || buflen == 0)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_plan_describe: null buffer");
+  const Plan *p = nullptr;
+  if (kind == KIND_C2C) {
+    if (stage < 0 || stage >= h->nstages)
+      return fail(B200FFT_ERR_INVALID_ARG, "b200fft_plan_describe: stage out of range");
+    p = &h->stages[stage];
+  } else if (kind == KIND_R2C) {
+    p = &h->r2c;
+  } else if (kind == KIND_C2R) {
+    p = &h->c2r;
+  } else {
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_plan_describe: bad kind");
+  }
+  if (!p->valid)
+    return fail(B200FFT_ERR_NO_PLAN, "b200fft_plan_describe: no such plan");
+  std::snprintf(buf, buflen, "%s", describe_choice(p->ch, p->kind).c_str());
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_export_wisdom(const char *path) {
+  if (path == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_export_wisdom: null path");
+  FILE *f = std::fopen(path, "w");
+  if (f == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, std::string("b200fft_export_wisdom: cannot write ") + path);
+  std::fprintf(f, "b200fft-wisdom 1\n");
+  {
+    std::lock_guard<std::mutex> lk(g_wis_mu);
+    for (const auto &kv : g_wisdom)
+      std::fprintf(f, "%s | %d %d %d %.6f\n", kv.first.c_str(), kv.second.family,
+                   kv.second.variant, kv.second.rigor, kv.second.ms);
+  }
+  std::fclose(f);
+  return B200FFT_SUCCESS;
+}
+
+int b200fft_import_wisdom(const char *path) {
+  if (path == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, "b200fft_import_wisdom: null path");
+  FILE *f = std::fopen(path, "r");
+  if (f == nullptr)
+    return fail(B200FFT_ERR_INVALID_ARG, std::string("b200fft_import_wisdom: cannot read ") + path);
+  char line[512];
+  int n = 0;
+  bool header = false;
+  while (std::fgets(line, sizeof(line), f)) {
+    std::string l(line);
+    while (!l.empty() && (l.back() == '\n' || l.back() == '\r'))
+      l.pop_back();
+    if (!header) {
+      header = l == "b200fft-wisdom 1";
+      if (!header) {
+        std::fclose(f);
+        return fail(B200FFT_ERR_INVALID_ARG, "b200fft_import_wisdom: not a wisdom file");
+      }
+      continue;
+    }
+    const size_t bar = l.find(" | ");
+    if (bar == std::string::npos)
+      continue;
+    WisdomVal v;
+    if (std::sscanf(l.c_str() + bar + 3, "%d %d %d %lf", &v.family, &v.variant, &v.rigor,
+                    &v.ms) != 4)
+      continue;
+    if (v.family < 0 || v.family > 1 || v.variant < 0 || v.variant >= kStaticVariants ||
+        v.rigor < 0 || v.rigor > 2)
+      continue;
+    std::lock_guard<std::mutex> lk(g_wis_mu);
+    g_wisdom[l.substr(0, bar)] = v;
+    ++n;
+  }
+  std::fclose(f);
+  return n;
+}
+
+int b200fft_forget_wisdom(void) {
+  std::lock_guard<std::mutex> lk(g_wis_mu);
+  g_wisdom.clear();
   return B200FFT_SUCCESS;
 }
 

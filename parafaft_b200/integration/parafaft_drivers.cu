@@ -104,6 +104,101 @@ template <int D, class B> struct R2CObj : Obj {
   }
 };
 
+// One-rank C2C transform driving a backend with the same call sequence as
+// ParaFaFT_C2C::forward/backward on one rank (parafaft_c2c.hpp:539-694):
+// plans per stage (last axis contiguous, first axis strided, middle axes one
+// slab per leading index, :249-287), a copy into the scratch buffer first when
+// D-1 is odd, then per stage the transform followed by the one-rank exchange
+// (a full-buffer copy, parafaft_common.hpp:488-494), ending in sync(). On one
+// rank every stage buffer has the global shape; ParaFaFT_C2C instead sizes
+// redistributed axes from another axis' extent (parafaft_c2c.hpp:826-831),
+// which is only right for hypercubic grids, so non-hypercubic grids are run
+// through this object.
+template <class B> b200fft_handle handle_of(const B &) { return nullptr; }
+template <class T> b200fft_handle handle_of(const parafaft::B200Backend<T> &b) {
+  return b.handle();
+}
+
+template <int D, class B> struct OneRankC2C : Obj {
+  using Cx = typename B::Complex;
+  B backend;
+  int shape[D];
+  std::size_t total = 1;
+  typename B::ComplexBuffer scratch;
+  OneRankC2C(const int *s, parafaft::FFTPlanFlag flag) : backend(D, flag) {
+    handle = handle_of(backend);
+    this->ndim = D;
+    for (int i = 0; i < D; ++i) {
+      shape[i] = s[i];
+      total *= static_cast<std::size_t>(s[i]);
+    }
+    scratch.resize(total);
+    for (int stage = 0; stage < D; ++stage) {
+      const int axis = D - 1 - stage;
+      const std::size_t n = static_cast<std::size_t>(shape[axis]);
+      std::size_t trailing = 1;
+      for (int i = axis + 1; i < D; ++i)
+        trailing *= static_cast<std::size_t>(shape[i]);
+      if (axis == D - 1)
+        backend.create_stage_plan(stage, shape[axis], total / n, scratch.data(), 1,
+                                  static_cast<std::ptrdiff_t>(n));
+      else if (axis == 0)
+        backend.create_stage_plan(stage, shape[axis], total / n, scratch.data(),
+                                  static_cast<std::ptrdiff_t>(total / n), 1);
+      else
+        backend.create_stage_plan(stage, shape[axis], trailing, scratch.data(),
+                                  static_cast<std::ptrdiff_t>(trailing), 1);
+    }
+  }
+  void stage_fft(int stage, parafaft::FFTDirection dir, Cx *buf) {
+    const int axis = D - 1 - stage;
+    if (axis == 0 || axis == D - 1) {
+      backend.execute_stage(stage, dir, buf);
+      return;
+    }
+    std::size_t leading = 1, slab = static_cast<std::size_t>(shape[axis]);
+    for (int i = 0; i < axis; ++i)
+      leading *= static_cast<std::size_t>(shape[i]);
+    for (int i = axis + 1; i < D; ++i)
+      slab *= static_cast<std::size_t>(shape[i]);
+    for (std::size_t i = 0; i < leading; ++i)
+      backend.execute_stage(stage, dir, buf + i * slab);
+  }
+  void run(Cx *data, bool fwd) {
+    Cx *src = data, *dst = scratch.data();
+    if ((D - 1) % 2 != 0) {
+      backend.memcpy(scratch.data(), data, total * sizeof(Cx));
+      src = scratch.data();
+      dst = data;
+    }
+    const auto dir = fwd ? parafaft::FFTDirection::Forward : parafaft::FFTDirection::Backward;
+    for (int k = 0; k < D; ++k) {
+      const int stage = fwd ? k : D - 1 - k;
+      stage_fft(stage, dir, src);
+      if (k < D - 1) {
+        backend.memcpy(dst, src, total * sizeof(Cx));
+        std::swap(src, dst);
+      }
+    }
+    backend.sync();
+  }
+  void forward(void *d) override { run(static_cast<Cx *>(d), true); }
+  void backward(void *d) override { run(static_cast<Cx *>(d), false); }
+  void forward_oop(const void *, void *) override {
+    throw std::runtime_error("out-of-place transforms exist for R2C objects only");
+  }
+  void backward_oop(void *, void *) override {
+    throw std::runtime_error("out-of-place transforms exist for R2C objects only");
+  }
+  long long required_size() const override { return static_cast<long long>(total); }
+  void shapes(int *a, int *b, int *c, int *d) const override {
+    for (int i = 0; i < D; ++i) {
+      a[i] = c[i] = shape[i];
+      b[i] = d[i] = 0;
+    }
+  }
+};
+
 template <template <int, class> class O, class B>
 Obj *make_d(int D, const int *shape, parafaft::FFTPlanFlag flag) {
   switch (D) {
@@ -146,13 +241,16 @@ extern "C" {
 
 const char *pfb_last_error(void) { return g_err.c_str(); }
 
-// kind: 0 C2C, 1 R2C. backend: 0 B200Backend, 1 CuFFTBackend. prec: B200FFT_F32/F64.
+// kind: 0 C2C (ParaFaFT_C2C), 1 R2C (ParaFaFT_R2C), 2 C2C through the
+// one-rank orchestrator above (any grid shape). backend: 0 B200Backend,
+// 1 CuFFTBackend. prec: B200FFT_F32/F64.
 int pfb_create(int kind, int D, int prec, int backend, const int *shape, int plan_flag,
                void **out) {
   return guard([&] {
     *out = nullptr;
-    Obj *o = kind == 0 ? make<C2CObj>(D, prec, backend, shape, plan_flag)
-                       : make<R2CObj>(D, prec, backend, shape, plan_flag);
+    Obj *o = kind == 0   ? make<C2CObj>(D, prec, backend, shape, plan_flag)
+             : kind == 1 ? make<R2CObj>(D, prec, backend, shape, plan_flag)
+                         : make<OneRankC2C>(D, prec, backend, shape, plan_flag);
     *out = o;
   });
 }

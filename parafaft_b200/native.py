@@ -41,6 +41,8 @@ ENGINE_SYMBOLS = (
     "b200fft_group_create", "b200fft_group_destroy", "b200fft_group_add",
     "b200fft_group_begin", "b200fft_group_end", "b200fft_group_capture",
     "b200fft_group_replay", "b200fft_group_sync", "b200fft_group_stats",
+    "b200fft_set_work_buffer", "b200fft_plan_describe", "b200fft_export_wisdom",
+    "b200fft_import_wisdom", "b200fft_forget_wisdom",
 )
 
 
@@ -118,6 +120,11 @@ def engine() -> C.CDLL:
             "b200fft_group_replay": (i, [vp]),
             "b200fft_group_sync": (i, [vp]),
             "b200fft_group_stats": (i, [vp, C.POINTER(Stats)]),
+            "b200fft_set_work_buffer": (i, [vp, vp, sz]),
+            "b200fft_plan_describe": (i, [vp, i, i, C.c_char_p, sz]),
+            "b200fft_export_wisdom": (i, [C.c_char_p]),
+            "b200fft_import_wisdom": (i, [C.c_char_p]),
+            "b200fft_forget_wisdom": (i, []),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -250,6 +257,14 @@ class Handle:
     def reset_stats(self):
         check(self._lib.b200fft_reset_stats(self._h))
 
+    def set_work_buffer(self, data, nbytes: int = 0):
+        check(self._lib.b200fft_set_work_buffer(self._h, _ptr(data), nbytes))
+
+    def plan_describe(self, kind: int = KIND_C2C, stage: int = 0) -> str:
+        buf = C.create_string_buffer(256)
+        check(self._lib.b200fft_plan_describe(self._h, kind, stage, buf, 256))
+        return buf.value.decode()
+
     def set_profiling(self, on: bool = True):
         check(self._lib.b200fft_set_profiling(self._h, 1 if on else 0))
 
@@ -328,6 +343,21 @@ def c2c_noalloc(precision: int, direction: int, length: int, batch: int, stride:
                                        _ptr(data_in), _ptr(data_out), stream or 0))
 
 
+def export_wisdom(path: str) -> None:
+    check(engine().b200fft_export_wisdom(str(path).encode()))
+
+
+def import_wisdom(path: str) -> int:
+    n = engine().b200fft_import_wisdom(str(path).encode())
+    if n < 0:
+        check(n)
+    return n
+
+
+def forget_wisdom() -> None:
+    check(engine().b200fft_forget_wisdom())
+
+
 def supported(precision: int, kind: int, length: int) -> bool:
     return bool(engine().b200fft_supported(precision, kind, length))
 
@@ -335,7 +365,9 @@ def supported(precision: int, kind: int, length: int) -> bool:
 class ParaFaFT:
     """A ParaFaFT_C2C<D, B> or ParaFaFT_R2C<D, B> object of the reference code.
 
-    kind: "c2c" or "r2c"; backend: "b200" (B200Backend<T>) or "cufft"
+    kind: "c2c" or "r2c" (the reference orchestrators), or "c2c_onerank" (the
+    same backend call sequence with per-axis extents, for grids that are not
+    hypercubic); backend: "b200" (B200Backend<T>) or "cufft"
     (the reference CuFFTBackend<T>, for comparison). Data arguments are device
     pointers (ints) or CUDA torch tensors.
     """
@@ -349,7 +381,8 @@ class ParaFaFT:
         self.precision = precision
         arr = (C.c_int * self.D)(*self.shape)
         h = C.c_void_p()
-        rc = self._lib.pfb_create(0 if kind == "c2c" else 1, self.D, precision,
+        kinds = {"c2c": 0, "r2c": 1, "c2c_onerank": 2}
+        rc = self._lib.pfb_create(kinds[kind], self.D, precision,
                                   0 if backend == "b200" else 1, arr, plan_flag, C.byref(h))
         if rc != 0:
             raise RuntimeError("ParaFaFT construction failed: " + self._lib.pfb_last_error().decode())

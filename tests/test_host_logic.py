@@ -179,3 +179,36 @@ st = g.stats()
 print(st["kernel_launches"], st["passes_per_run"], st["copies_issued"])
 ''')
     assert out.split() == ["6", str(256 * 6), "0"]
+
+
+def test_wisdom_roundtrip_and_plan_choice(tmp_path):
+    """Wisdom entries choose the kernel of later plans of the same geometry;
+    export/import/forget round-trip through a text file (record-only handles,
+    so nothing is timed)."""
+    nv.forget_wisdom()
+    w = tmp_path / "w.txt"
+    # a hand-written entry: 512-point column plan, generic kernel, Patient rigor
+    w.write_text("b200fft-wisdom 1\n"
+                 "record-only p0 k0 n512 b131584 s131584 d1 l1 | 1 0 2 0.1\n"
+                 "record-only p0 k0 n512 b257 s257 d1 l1 | 0 3 1 0.2\n"
+                 "garbage line\n")
+    assert nv.import_wisdom(w) == 2
+    h = nv.Handle(nv.F32, 3, plan_flag=nv.PLAN_MEASURE, flags=nv.FLAG_RECORD_ONLY)
+    h.plan_c2c(2, 512, 131584, 131584, 1)
+    assert h.plan_describe(nv.KIND_C2C, 2).startswith("generic c2c L=512")
+    h.plan_c2c(1, 512, 257, 257, 1)   # lead inferred 512 from stage 2 -> key l512: no entry
+    assert "var=0" in h.plan_describe(nv.KIND_C2C, 1)
+    e = nv.Handle(nv.F32, 3, plan_flag=nv.PLAN_ESTIMATE, flags=nv.FLAG_RECORD_ONLY)
+    e.plan_c2c(2, 512, 131584, 131584, 1)  # Estimate does not consult wisdom
+    assert e.plan_describe(nv.KIND_C2C, 2).startswith("static c2c L=512")
+    out = tmp_path / "out.txt"
+    nv.export_wisdom(out)
+    lines = out.read_text().splitlines()
+    assert lines[0] == "b200fft-wisdom 1" and len(lines) == 3
+    nv.forget_wisdom()
+    nv.export_wisdom(out)
+    assert out.read_text().splitlines() == ["b200fft-wisdom 1"]
+    bad = tmp_path / "bad.txt"
+    bad.write_text("not wisdom\n")
+    with pytest.raises(nv.B200FFTError):
+        nv.import_wisdom(bad)

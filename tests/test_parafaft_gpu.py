@@ -186,3 +186,31 @@ def test_golden_fixtures_on_gpu():
             y = to_host(d)[:p.size].view(np.complex128).reshape(case["output"].shape)
         assert O.max_abs(y, case["output"]) < ABS_F64, case["name"]
         assert O.rel_l2(y, case["output"]) < 1e-12, case["name"]
+
+
+@pytest.mark.parametrize("flag", [nv.PLAN_MEASURE, nv.PLAN_PATIENT])
+def test_measured_plans(flag, tmp_path):
+    """FFTPlanFlag::Measure/Patient: candidates are timed on ParaFaFT's scratch
+    buffer at construction; the chosen kernels give the same results and the
+    choices land in the plan cache (wisdom)."""
+    _drivers_or_skip()
+    nv.forget_wisdom()
+    shape = (64, 96, 128)
+    x = O.normal_real(shape, 31)
+    f = nv.ParaFaFT("r2c", shape, nv.F32, plan_flag=flag)
+    buf = np.zeros(f.required_size, np.float32)
+    p = O.pad_real(x, np.float32)
+    buf[:p.size] = p
+    d = to_dev(buf)
+    f.forward(d)
+    X = to_host(d)[:p.size].view(np.complex64).reshape(64, 96, 65)
+    assert O.rel_l2(X, O.r2c_nd(x)) < 2e-6
+    w = tmp_path / "w.txt"
+    nv.export_wisdom(w)
+    entries = w.read_text().splitlines()[1:]
+    assert len(entries) >= 3  # r2c, c2r and the two column stages (c2r may share)
+    # a second object of the same geometry reuses the entries
+    g = nv.ParaFaFT("r2c", shape, nv.F32, plan_flag=flag)
+    h1, h2 = f.handle(), g.handle()
+    for stage in (1, 2):
+        assert h1.plan_describe(nv.KIND_C2C, stage) == h2.plan_describe(nv.KIND_C2C, stage)
