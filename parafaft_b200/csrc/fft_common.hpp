@@ -146,15 +146,22 @@ constexpr int ce_max(int a, int b) { return a > b ? a : b; }
 //       point row is read as one longer contiguous segment;
 //   4 = staged column pass: persistent CTAs of 512 threads, full tile,
 //       cp.async double buffering (one CTA per SM);
-//   5 = full column tile on 512 threads (half the points per thread).
-constexpr int kStaticVariants = 6;
+//   5 = full column tile on 512 threads (half the points per thread);
+//   6 = pipelined column pass: persistent CTAs of 256 threads on half tiles,
+//       the next tile's points loaded into a second register set while the
+//       current one is transformed (two CTAs per SM).
+constexpr int kStaticVariants = 7;
 constexpr int kVariantStaged = 4;
+constexpr int kVariantPipelined = 6;
 
 constexpr CfgS cfg_static(int esize, int L, bool col, int variant = 0) {
-  const int NT = (col && (variant >= 3)) ? 512 : 256;
+  const int NT = (col && (variant >= 3 && variant <= 5)) ? 512 : 256;
   const int base = esize == 8 ? 8192 : 4096;
-  const int target =
-      col ? (variant == 3 ? 2 * base : (variant >= 4 ? base : (base >> variant))) : base;
+  const int target = col ? (variant == 3 ? 2 * base
+                                         : (variant == 4 || variant == 5)
+                                               ? base
+                                               : variant == 6 ? base / 2 : (base >> variant))
+                         : base;
   const int emax = esize == 8 ? 32 : 16;
   if (col) {
     int TB = ce_min(NT, ce_max(1, target / L));

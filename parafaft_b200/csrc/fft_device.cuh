@@ -526,6 +526,69 @@ struct KS {
     run<0>(c, v);
   }
 
+  // ---- persistent column pass with register prefetch ----------------------
+  // Each CTA walks tiles blockIdx.x, +gridDim.x, ...; the points of the next
+  // tile are loaded into a second register set before the current tile is
+  // transformed, so global loads stay in flight through the compute phase.
+  // Shared memory holds one exchange buffer per register set.
+  static BF_D void set_tile(Ctx &c, const PassArgs &a, long long tile) {
+    const long long b = tile * TB + c.tb;
+    c.act = b < a.total;
+    long long ioff = 0, ooff = 0;
+    if (c.act) {
+      const long long sl = b / a.batch;
+      const long long w = b - sl * a.batch;
+      ioff = sl * a.islab + w * a.idist;
+      ooff = sl * a.oslab + w * a.odist;
+    }
+    c.gin = reinterpret_cast<const V *>(a.in) + ioff;
+    c.gout = reinterpret_cast<V *>(a.out) + ooff;
+  }
+  static BF_D void load_first(const Ctx &c, V (&v)[EMAX]) {
+    constexpr int R = S.rad[0];
+    constexpr int B = L / R;
+    constexpr int K = (B + P - 1) / P;
+    constexpr bool FULL = (B % P) == 0;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      const int j = c.g + P * i;
+      const bool ok = c.act && (FULL || j < B);
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        v[i * R + r] = ok ? c.gin[(long long)(j + r * B) * c.ist] : czero<V>();
+    }
+  }
+  static BF_D void entry_pipelined(const PassArgs &a, V *smem) {
+    static_assert(COL && KIND == KIND_C2C, "pipelined path is for column C2C");
+    const long long ntiles = (a.total + TB - 1) / TB;
+    const long long G = gridDim.x;
+    long long t = blockIdx.x;
+    if (t >= ntiles)
+      return;
+    Ctx ca, cb;
+    const int tid = threadIdx.x;
+    ca.g = cb.g = tid / TB;
+    ca.tb = cb.tb = tid % TB;
+    ca.tw = cb.tw = reinterpret_cast<const V *>(a.tw);
+    ca.ist = cb.ist = a.istride;
+    ca.ost = cb.ost = a.ostride;
+    ca.sm = smem;
+    cb.sm = smem + static_cast<size_t>(L) * TB;
+    V va[EMAX], vb[EMAX];
+    set_tile(ca, a, t);
+    load_first(ca, va);
+    for (; t < ntiles; t += 2 * G) {
+      set_tile(cb, a, t + G); // inactive (no loads) past the last tile
+      load_first(cb, vb);
+      run<0>(ca, va);
+      if (t + G >= ntiles)
+        break;
+      set_tile(ca, a, t + 2 * G);
+      load_first(ca, va);
+      run<0>(cb, vb);
+    }
+  }
+
   // ---- persistent column pass with cp.async double buffering -------------
   // CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ...; while tile t is
   // transformed in one shared buffer, the points of the next tile stream into
@@ -616,6 +679,14 @@ __global__ void __launch_bounds__(NT, (COL && NT == 256) ? B2_COL_MIN_BLOCKS : 1
   using K = KS<T, L, NT, TB, COL, FWD, KIND>;
   extern __shared__ __align__(16) unsigned char smraw[];
   K::entry(a, reinterpret_cast<typename K::V *>(smraw));
+}
+
+template <typename T, int L, int NT, int TB, bool FWD>
+__global__ void __launch_bounds__(NT, 2)
+    fft_static_pipelined_kernel(const PassArgs a) {
+  using K = KS<T, L, NT, TB, true, FWD, KIND_C2C>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  K::entry_pipelined(a, reinterpret_cast<typename K::V *>(smraw));
 }
 
 template <typename T, int L, int NT, int TB, bool FWD>

@@ -80,11 +80,38 @@ cudaError_t launch_static_staged(const PassArgs &a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+template <typename T, int L, bool FWD>
+cudaError_t launch_static_pipelined(const PassArgs &a, cudaStream_t st) {
+  constexpr CfgS cf = cfg_static(static_cast<int>(sizeof(cvec<T>)), L, true, kVariantPipelined);
+  using K = KS<T, L, cf.NT, cf.TB, true, FWD, KIND_C2C>;
+  auto kern = fft_static_pipelined_kernel<T, L, cf.NT, cf.TB, FWD>;
+  constexpr size_t smem = 2 * K::smem_bytes();
+  static int configured_mask = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (smem > 48 * 1024 && dev >= 0 && dev < 31 && !(configured_mask & (1 << dev))) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess)
+      return e;
+    configured_mask |= (1 << dev);
+  }
+  const long long ntiles = (a.total + cf.TB - 1) / cf.TB;
+  if (ntiles <= 0)
+    return cudaSuccess;
+  const long long slots = static_cast<long long>(sm_count()) * 2;
+  const long long grid = ntiles < slots ? ntiles : slots;
+  kern<<<static_cast<unsigned>(grid), cf.NT, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
 template <typename T, int L, bool COL, bool FWD, int KIND>
 cudaError_t launch_static_var(int var, const PassArgs &a, cudaStream_t st) {
   if constexpr (COL && KIND == KIND_C2C) {
     if (var == kVariantStaged)
       return launch_static_staged<T, L, FWD>(a, st);
+    if (var == kVariantPipelined)
+      return launch_static_pipelined<T, L, FWD>(a, st);
   }
   switch (var) {
   case 1: return launch_static_one<T, L, COL, FWD, KIND, 1>(a, st);
