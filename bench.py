@@ -321,6 +321,7 @@ def run_c2c_config(args):
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
         "dtype": prec_s, "data": f"synthetic {dist} complex, seed {seed}",
         "config": {"workload": f"{kind} {'x'.join(map(str, shape))} {prec_s}", "orchestrator": kind},
+        "form": args.form,
         "rel_l2_fwd": rel_fwd, "rel_l2_reference": ref_src, "rel_l2_roundtrip": rel_rt,
         "alg_bytes": alg, "hbm_frac": round(alg / (ms * 1e-3) / 1e9 / peak, 4),
         "peak_source": peak_kind, "kernels": kernels,
@@ -631,7 +632,12 @@ def main():
                          "uneven grids; c2c64 / c2c1024 / c2c4d: the C2C configurations")
     ap.add_argument("--grids", type=int, default=256)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--form", default="plain", choices=["plain", "split-tc"],
+                    help="split-tc: FP32 C2C passes of length 256/512/1024 use the "
+                         "split-precision tensor-core kernels (FP16 hi+lo, FP32 accumulate)")
     args = ap.parse_args()
+    if args.form == "split-tc":
+        os.environ["B200FFT_SPLIT_TC"] = "1"  # read when each backend handle is created
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     if args.impl == "reference":

@@ -67,6 +67,11 @@ extern "C" {
 #define B200FFT_FLAG_NO_DEFER 1u   /* issue every call at once: no fusion   */
 #define B200FFT_FLAG_RECORD_ONLY 2u /* plan and account, never touch a GPU  */
 #define B200FFT_FLAG_GENERIC_ONLY 4u /* force the runtime-generic kernels    */
+/* FP32 C2C plans of length 256, 512 and 1024 use the split-precision
+ * tensor-core kernels: radix-16 DFT blocks as FP16 hi+lo matrix products
+ * with FP32 accumulation (relative L2 error within twice the plain FP32
+ * kernels'). Other plans are unaffected. Also set by B200FFT_SPLIT_TC=1. */
+#define B200FFT_FLAG_SPLIT_TC 8u
 
 typedef struct b200fft_handle_s *b200fft_handle;
 

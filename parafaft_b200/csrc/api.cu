@@ -63,7 +63,7 @@ bool env_flag(const char *name) {
 
 // Kernel choice of a plan.
 struct Choice {
-  int family = 0; // 0 static, 1 generic
+  int family = 0; // 0 static, 1 generic, 2 split-precision tensor core
   bool col = false;
   int L = 0;      // complex points of the stage loop
   int tlen = 0;   // twiddle table length
@@ -160,8 +160,11 @@ int default_variant(int csize, int L, bool col, long long stride) {
 
 // Choose the kernel for a plan. kind: KIND_C2C/R2C/C2R. `variant` >= 0 asks
 // for that tile-shape candidate of the specialised kernel (else the default).
+// split_tc asks for the split-precision tensor-core kernels where they exist
+// (FP32 C2C of length 256, 512 or 1024).
 int choose_kernel(int prec, int kind, int len, long long batch, long long stride,
-                  long long dist, bool force_generic, Choice *out, int variant = -1) {
+                  long long dist, bool force_generic, Choice *out, int variant = -1,
+                  bool split_tc = false) {
   const int csize = prec == B200FFT_F64 ? 16 : 8;
   Choice ch;
   int L = len;
@@ -176,6 +179,15 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
     ch.tlen = len;
   }
   ch.L = L;
+  if (split_tc && !force_generic && prec == B200FFT_F32 && kind == KIND_C2C &&
+      tc_length_ok(L)) {
+    ch.family = 2;
+    ch.variant = 0;
+    ch.TB = ch.col ? 16 : 4;
+    ch.NT = ch.col ? (L == 1024 ? 512 : 256) : 128;
+    *out = ch;
+    return B200FFT_SUCCESS;
+  }
   const bool static_ok =
       !force_generic && static_length_ok(L) &&
       (kind == KIND_C2C || (!odd && stride == 1 && dist % 2 == 0 && L <= 2048));
@@ -242,7 +254,9 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
 std::string describe_choice(const Choice &ch, int kind) {
   char buf[256];
   std::string rad;
-  if (ch.family == 0) {
+  if (ch.family == 2) {
+    rad = (ch.L > 256 ? std::to_string(ch.L / 256) + "x" : std::string()) + "16x16";
+  } else if (ch.family == 0) {
     int m = ch.L;
     std::vector<int> r;
     while (m % 8 == 0 && m > 1) { r.push_back(8); m /= 8; }
@@ -258,7 +272,7 @@ std::string describe_choice(const Choice &ch, int kind) {
     rad = "1";
   const char *kn = kind == KIND_C2C ? "c2c" : (kind == KIND_R2C ? "r2c" : "c2r");
   std::snprintf(buf, sizeof(buf), "%s %s L=%d %s tb=%d nt=%d radices=%s var=%d",
-                ch.family == 0 ? "static" : "generic", kn, ch.L,
+                ch.family == 0 ? "static" : (ch.family == 2 ? "split-tc" : "generic"), kn, ch.L,
                 ch.col ? "col" : "row", ch.TB, ch.NT, rad.c_str(), ch.variant);
   return buf;
 }
@@ -282,6 +296,7 @@ struct b200fft_handle_s {
   bool record_only = false;
   bool defer = true;
   bool force_generic = false;
+  bool split_tc = false; // split-precision tensor-core kernels where they exist
   int device = -1;
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
@@ -646,6 +661,8 @@ cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
     else
       e = f64 ? launch_static_c2r_f64(p.ch.L, p.ch.variant, a, h->stream)
               : launch_static_c2r_f32(p.ch.L, p.ch.variant, a, h->stream);
+  } else if (p.ch.family == 2) {
+    e = launch_tc_c2c_f32(p.ch.L, p.ch.col, fwd, a, h->stream);
   } else {
     GenArgs g = p.ch.gen;
     g.p = a;
@@ -866,12 +883,14 @@ int make_plan(H *h, Plan *dst, int kind, int length, size_t batch,
   p.stride = stride;
   p.dist = dist;
   B2_TRY(choose_kernel(h->prec, kind, length, p.batch, stride, dist,
-                       h->force_generic, &p.ch));
+                       h->force_generic, &p.ch, -1, h->split_tc));
   const void *tw = nullptr;
   B2_TRY(get_table(h, p.ch.tlen, &tw));
   p.valid = true;
   *dst = p; // visible to infer_lead while tuning
-  if (h->plan_flag >= B200FFT_PLAN_MEASURE && !h->force_generic &&
+  // The split-precision kernels are a precision choice, not a tuning
+  // candidate: plans that use them are not timed against the plain ones.
+  if (h->plan_flag >= B200FFT_PLAN_MEASURE && !h->force_generic && p.ch.family != 2 &&
       std::getenv("B200FFT_VARIANT") == nullptr) {
     B2_TRY(autotune(h, p));
     *dst = p;
@@ -949,6 +968,8 @@ int b200fft_create(int precision, int num_stages, int plan_flag, unsigned flags,
     flags |= B200FFT_FLAG_NO_DEFER;
   if (env_flag("B200FFT_GENERIC_ONLY"))
     flags |= B200FFT_FLAG_GENERIC_ONLY;
+  if (env_flag("B200FFT_SPLIT_TC"))
+    flags |= B200FFT_FLAG_SPLIT_TC;
   static std::once_flag wisdom_once; // B200FFT_WISDOM=path: import once per process
   std::call_once(wisdom_once, [] {
     if (const char *w = std::getenv("B200FFT_WISDOM"))
@@ -964,6 +985,7 @@ int b200fft_create(int precision, int num_stages, int plan_flag, unsigned flags,
   h->record_only = (flags & B200FFT_FLAG_RECORD_ONLY) != 0;
   h->defer = (flags & B200FFT_FLAG_NO_DEFER) == 0;
   h->force_generic = (flags & B200FFT_FLAG_GENERIC_ONLY) != 0;
+  h->split_tc = (flags & B200FFT_FLAG_SPLIT_TC) != 0;
   h->stages.resize(num_stages);
   if (!h->record_only) {
     int n = 0;

@@ -22,6 +22,7 @@ F32, F64 = 0, 1
 FORWARD, BACKWARD = 0, 1
 PLAN_ESTIMATE, PLAN_MEASURE, PLAN_PATIENT = 0, 1, 2
 FLAG_NO_DEFER, FLAG_RECORD_ONLY, FLAG_GENERIC_ONLY = 1, 2, 4
+FLAG_SPLIT_TC = 8  # split-precision tensor-core C2C (FP32, lengths 256/512/1024)
 KIND_C2C, KIND_R2C, KIND_C2R = 0, 1, 2
 
 STATUS = {

@@ -63,6 +63,30 @@ def test_kernel_selection(kind, n, expect):
     assert nv.describe(nv.F32, kind, n).startswith(expect)
 
 
+def test_split_tc_selection():
+    """FLAG_SPLIT_TC selects the tensor-core kernels for FP32 C2C of length
+    256/512/1024 (row and column tiles) and leaves every other plan alone."""
+    h = nv.Handle(nv.F32, 4, flags=nv.FLAG_RECORD_ONLY | nv.FLAG_SPLIT_TC)
+    h.plan_c2c(0, 1024, 100, 1, 1024)
+    h.plan_c2c(1, 512, 300, 300, 1)
+    h.plan_c2c(2, 2048, 10, 1, 2048)
+    h.plan_c2c(3, 256, 7, 7, 1)
+    assert h.plan_describe(nv.KIND_C2C, 0).startswith(
+        "split-tc c2c L=1024 row tb=4 nt=128 radices=4x16x16")
+    assert h.plan_describe(nv.KIND_C2C, 1).startswith(
+        "split-tc c2c L=512 col tb=16 nt=256 radices=2x16x16")
+    assert h.plan_describe(nv.KIND_C2C, 2).startswith("static c2c L=2048")
+    assert h.plan_describe(nv.KIND_C2C, 3).startswith(
+        "split-tc c2c L=256 col tb=16 nt=256 radices=16x16")
+    h.plan_r2c(512, 4, 1, 514)
+    assert h.plan_describe(nv.KIND_R2C, 0).startswith("static r2c L=256")
+    d = nv.Handle(nv.F64, 1, flags=nv.FLAG_RECORD_ONLY | nv.FLAG_SPLIT_TC)
+    d.plan_c2c(0, 1024, 100, 1, 1024)
+    assert d.plan_describe(nv.KIND_C2C, 0).startswith("static c2c L=1024")
+    h.plan_c2c(1, 1024, 64, 64, 1)  # a 1024-point column tile uses 16 warps
+    assert h.plan_describe(nv.KIND_C2C, 1).startswith("split-tc c2c L=1024 col tb=16 nt=512")
+
+
 def test_supported_lengths():
     assert nv.supported(nv.F32, nv.KIND_C2C, 4096)
     assert nv.supported(nv.F64, nv.KIND_R2C, 3 * 7 * 61)
