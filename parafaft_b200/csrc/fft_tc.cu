@@ -35,9 +35,7 @@
 // (k1 in {g, g+8}, n2 in {2t, 2t+1} + 8j) are register for register the B
 // fragments of step 2 (vectors k1, slots n2), so the corner turn of the
 // four-step moves no data; the outputs k = 2t + h + 8jp + 16 (g + 8hh) leave
-// as contiguous 16-byte stores. One block exponent per 256-point block. The
-// next transform of the warp is staged in shared memory by cp.async while the
-// current one is transformed.
+// as contiguous 16-byte stores. One block exponent per 256-point block.
 //
 // Column transforms (points strided, neighbouring transforms adjacent): a
 // CTA takes 16 neighbouring transforms, so every point row is one 128-byte
@@ -207,71 +205,41 @@ BF_D void row_w256(const TcConst &K, const float2 *tw256, float2 (&x)[8], int g,
   }
 }
 
-// Per-warp shared-memory slot of point e of a row transform: the contiguous
-// layout with 16-byte chunks swizzled so that the contiguous staging copies
-// and the fragment-order reads (lanes at points 32t + g + const) are both
-// free of bank conflicts.
-BF_D int rswz(int e) {
-  const int m2 = ((e >> 5) ^ (e >> 9)) & 1;
-  const int m3 = ((e >> 6) ^ (e >> 4) ^ (e >> 8)) & 1;
-  return e ^ (m2 << 2) ^ (m3 << 3);
-}
-
 // 512- and 1024-point rows hold 16 and 32 points per lane: three 4-warp CTAs
 // per SM leave them room.
 template <int L> constexpr int row_min_blocks() { return L >= 512 ? 3 : 4; }
 constexpr int kRowWarps = 4;
-template <int L> constexpr size_t row_smem() {
-  return static_cast<size_t>(kRowWarps) * 2 * L * sizeof(float2);
-}
 
-// Stage row transform b into dst with cp.async (coalesced: lane-contiguous).
-template <int L>
-BF_D void row_prefetch(const PassArgs &a, long long b, float2 *dst, int lane) {
-  const long long sl = b / a.batch, w = b - sl * a.batch;
-  const float2 *in = static_cast<const float2 *>(a.in) + sl * a.islab + w * a.idist;
-#pragma unroll 8
-  for (int k = 0; k < L / 32; ++k) {
-    const int e = lane + 32 * k;
-    cp_async_elem(dst + rswz(e), in + e * a.istride);
-  }
-}
-
-// Each warp walks transforms b, b + (all warps), ...; the next transform is
-// copied into the warp's second buffer (cp.async) while the current one is
-// transformed, so HBM reads stay in flight through the tensor-core work.
+// Each warp walks transforms b, b + (all warps), ...: it loads the points of
+// its fragments straight from global memory (every load instruction covers
+// full 32-byte sectors), transforms them in registers and stores 16-byte
+// runs of the output.
 template <int L, bool FWD>
 __global__ void __launch_bounds__(kRowWarps * 32, row_min_blocks<L>())
     fft_tc_row_kernel(PassArgs a) {
   constexpr int R0 = L / 256;
-  extern __shared__ __align__(16) unsigned char tc_smraw[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
-  float2 *buf = reinterpret_cast<float2 *>(tc_smraw) + static_cast<size_t>(warp) * 2 * L;
   const float2 *tw = static_cast<const float2 *>(a.tw);
   const float2 *tw256 = tw + (2 * L - 512); // pyramid level n at offset 2L - 2n
   TcConst K;
   tc_setup<FWD>(K, tw + (2 * L - 32), g, t);
   const long long nwarp = static_cast<long long>(gridDim.x) * kRowWarps;
-  long long b = static_cast<long long>(blockIdx.x) * kRowWarps + warp;
-  if (b < a.total)
-    row_prefetch<L>(a, b, buf, lane);
-  cp_async_commit();
 #pragma unroll 1
-  for (int it = 0; b < a.total; ++it, b += nwarp) {
-    if (b + nwarp < a.total)
-      row_prefetch<L>(a, b + nwarp, buf + ((it + 1) & 1) * L, lane);
-    cp_async_commit();
-    cp_async_wait<1>();
-    __syncwarp();
-    const float2 *cur = buf + (it & 1) * L;
+  for (long long b = static_cast<long long>(blockIdx.x) * kRowWarps + (threadIdx.x >> 5);
+       b < a.total; b += nwarp) {
+    const long long sl = b / a.batch, w = b - sl * a.batch;
+    const float2 *in = static_cast<const float2 *>(a.in) + sl * a.islab + w * a.idist;
+    float2 *out = static_cast<float2 *>(a.out) + sl * a.oslab + w * a.odist;
+    const long long is = a.istride, os = a.ostride;
     float2 x[R0][8];
 #pragma unroll
     for (int q = 0; q < R0; ++q)
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const int j = i >> 2, r = (i >> 1) & 1, h = i & 1;
-        x[q][i] = cur[rswz(256 * q + 16 * (2 * t + h + 8 * r) + g + 8 * j)];
+        const int n = 256 * q + 16 * (2 * t + h + 8 * r) + g + 8 * j;
+        x[q][i] = in[n * is];
       }
     if constexpr (R0 > 1) {
 #pragma unroll
@@ -291,9 +259,6 @@ __global__ void __launch_bounds__(kRowWarps * 32, row_min_blocks<L>())
 #pragma unroll
     for (int p = 0; p < R0; ++p)
       row_w256<FWD>(K, tw256, x[p], g, t);
-    const long long sl = b / a.batch, w = b - sl * a.batch;
-    float2 *out = static_cast<float2 *>(a.out) + sl * a.oslab + w * a.odist;
-    const long long os = a.ostride;
     // X[R0 k + p] with k = 2t + h + 8jp + 16 (g + 8hh): for each (jp, hh) the
     // lane holds 2 R0 consecutive outputs starting at R0 (2t + 8jp + 16 (g + 8hh)).
     const bool vec = os == 1 && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
@@ -319,9 +284,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, row_min_blocks<L>())
               out[(R0 * (k0 + h) + p) * os] = x[p][jp * 4 + hh * 2 + h];
         }
       }
-    __syncwarp(); // `cur` is refilled by the next iteration's prefetch
   }
-  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -574,14 +537,14 @@ template <int L, bool FWD> cudaError_t launch_row(const PassArgs &a, cudaStream_
   auto kern = fft_tc_row_kernel<L, FWD>;
   static int mask = 0, per_sm[32] = {0};
   int slots = 0;
-  const cudaError_t e = prepare(kern, kRowWarps * 32, row_smem<L>(), &slots, &mask, per_sm);
+  const cudaError_t e = prepare(kern, kRowWarps * 32, 0, &slots, &mask, per_sm);
   if (e != cudaSuccess)
     return e;
   const long long blocks = (a.total + kRowWarps - 1) / kRowWarps;
   if (blocks <= 0)
     return cudaSuccess;
   const long long grid = blocks < slots ? blocks : slots;
-  kern<<<static_cast<unsigned>(grid), kRowWarps * 32, row_smem<L>(), st>>>(a);
+  kern<<<static_cast<unsigned>(grid), kRowWarps * 32, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -620,7 +583,7 @@ cudaError_t launch_tc_c2c_f32(int L, bool col, bool fwd, const PassArgs &a, cuda
 }
 
 size_t tc_smem_bytes(int L, bool col) {
-  return col ? static_cast<size_t>(L) * 16 * 8 : static_cast<size_t>(kRowWarps) * 2 * L * 8;
+  return col ? static_cast<size_t>(L) * 16 * 8 : 0;
 }
 
 } // namespace b200fft
