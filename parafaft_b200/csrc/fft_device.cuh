@@ -467,8 +467,10 @@ struct KS {
     c.gin = reinterpret_cast<const V *>(a.in) + ioff;
     c.gout = reinterpret_cast<V *>(a.out) + ooff;
     c.tw = reinterpret_cast<const V *>(a.tw);
-    c.ist = a.istride;
-    c.ost = a.ostride;
+    // R2C/C2R rows are contiguous (unit stride, checked by the planner): a
+    // constant stride lets every load and store fold its offset.
+    c.ist = KIND == KIND_C2C ? a.istride : 1;
+    c.ost = KIND == KIND_C2C ? a.ostride : 1;
     c.sm = sm;
 
     V v[EMAX];
@@ -673,8 +675,11 @@ struct KS {
 #ifndef B2_COL_MIN_BLOCKS
 #define B2_COL_MIN_BLOCKS 2
 #endif
+#ifndef B2_ROW_MIN_BLOCKS
+#define B2_ROW_MIN_BLOCKS 2
+#endif
 template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND>
-__global__ void __launch_bounds__(NT, (COL && NT == 256) ? B2_COL_MIN_BLOCKS : 1)
+__global__ void __launch_bounds__(NT, NT == 256 ? (COL ? B2_COL_MIN_BLOCKS : B2_ROW_MIN_BLOCKS) : 1)
     fft_static_kernel(const PassArgs a) {
   using K = KS<T, L, NT, TB, COL, FWD, KIND>;
   extern __shared__ __align__(16) unsigned char smraw[];
