@@ -149,12 +149,15 @@ int ilog2(int x) {
 
 // Tile-shape candidate used without autotuning. Column passes whose points
 // lie 4 MiB or more apart (the first axis of large grids) read wider
-// contiguous segments per point row with the wide tile; everything else uses
-// the full tile (measured on the 512^3 and 1024^3 passes).
+// contiguous segments per point row with the wide tile; other FP32 columns of
+// 512 or more points use the 512-thread full tile; everything else the full
+// tile (measured on the 512^3 and 1024^3 passes).
 int default_variant(int csize, int L, bool col, long long stride) {
-  (void)L;
   if (col && stride * csize >= (4ll << 20))
     return 3;
+  // FP32 columns of 512+ points: 512-thread full tiles, two CTAs per SM
+  if (col && csize == 8 && L >= 512)
+    return 5;
   return 0;
 }
 
@@ -816,8 +819,8 @@ int autotune(H *h, Plan &p) {
   std::vector<std::pair<int, int>> cands; // (family, variant)
   if (p.ch.family == 0) {
     if (p.ch.col) {
-      const int meas[] = {0, 3, 1};
-      const int pat[] = {0, 1, 2, 3, 4, 5};
+      const int meas[] = {0, 3, 5};
+      const int pat[] = {0, 1, 2, 3, 4, 5, 6};
       if (rigor >= B200FFT_PLAN_PATIENT)
         for (int v : pat) cands.push_back({0, v});
       else

@@ -678,8 +678,14 @@ struct KS {
 #ifndef B2_ROW_MIN_BLOCKS
 #define B2_ROW_MIN_BLOCKS 2
 #endif
+// 512-thread FP32 column tiles with at most 16 points per thread fit two
+// CTAs per SM (64 registers; FP64 points need twice the registers).
+template <int ES, int NT, int TB, int L, bool COL> constexpr int static_min_blocks() {
+  return NT == 256 ? (COL ? B2_COL_MIN_BLOCKS : B2_ROW_MIN_BLOCKS)
+                   : ((ES == 8 && COL && NT == 512 && (TB * L) / NT <= 16) ? 2 : 1);
+}
 template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND>
-__global__ void __launch_bounds__(NT, NT == 256 ? (COL ? B2_COL_MIN_BLOCKS : B2_ROW_MIN_BLOCKS) : 1)
+__global__ void __launch_bounds__(NT, (static_min_blocks<int(sizeof(T) * 2), NT, TB, L, COL>()))
     fft_static_kernel(const PassArgs a) {
   using K = KS<T, L, NT, TB, COL, FWD, KIND>;
   extern __shared__ __align__(16) unsigned char smraw[];

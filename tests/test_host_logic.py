@@ -221,7 +221,7 @@ def test_wisdom_roundtrip_and_plan_choice(tmp_path):
     h.plan_c2c(2, 512, 131584, 131584, 1)
     assert h.plan_describe(nv.KIND_C2C, 2).startswith("generic c2c L=512")
     h.plan_c2c(1, 512, 257, 257, 1)   # lead inferred 512 from stage 2 -> key l512: no entry
-    assert "var=0" in h.plan_describe(nv.KIND_C2C, 1)
+    assert "var=5" in h.plan_describe(nv.KIND_C2C, 1)  # the default tile
     e = nv.Handle(nv.F32, 3, plan_flag=nv.PLAN_ESTIMATE, flags=nv.FLAG_RECORD_ONLY)
     e.plan_c2c(2, 512, 131584, 131584, 1)  # Estimate does not consult wisdom
     assert e.plan_describe(nv.KIND_C2C, 2).startswith("static c2c L=512")
