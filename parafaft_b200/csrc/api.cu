@@ -224,7 +224,7 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
                     " exceeds the single-pass limit of the generic kernel");
   int TB = 1;
   const size_t target = 48 * 1024;
-  while (TB < 64 && one * (2 * TB) <= target)
+  while (TB < kGenMaxTB && one * (2 * TB) <= target)
     TB *= 2;
   g.L = L;
   g.nreal = kind == KIND_C2C ? 0 : len;

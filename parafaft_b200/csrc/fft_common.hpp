@@ -60,6 +60,9 @@ inline FastDiv make_fastdiv(uint32_t d) {
 constexpr int kGenMaxStages = 24;
 constexpr int kGenMaxPrime = 61; // largest prime radix done by direct DFT
 constexpr int kGenThreads = 256;
+constexpr int kGenMaxTB = 64; // transforms per generic tile at most
+// static shared memory of a generic tile: input and output offsets per transform
+constexpr int kGenStaticSmem = 2 * kGenMaxTB * 8;
 
 struct GenArgs {
   PassArgs p;

@@ -772,18 +772,30 @@ BF_D void gen_tile(const GenArgs &a, long long tile, unsigned char *smraw) {
   const int TB = a.TB, L = a.L;
   const long long tile0 = tile * TB;
 
+  // Offsets of the tile's transforms, computed once per tile (one 64-bit
+  // division each) instead of once per element. -1: beyond the batch.
+  __shared__ long long s_io[kGenMaxTB], s_oo[kGenMaxTB];
+  if (tid < TB) {
+    const long long b = tile0 + tid;
+    long long io = -1, oo = -1;
+    if (b < a.p.total) {
+      const long long sl = b / a.p.batch;
+      const long long w = b - sl * a.p.batch;
+      io = sl * a.p.islab + w * a.p.idist;
+      oo = sl * a.p.oslab + w * a.p.odist;
+    }
+    s_io[tid] = io;
+    s_oo[tid] = oo;
+  }
+  __syncthreads();
   auto offsets = [&](int tb, long long &io, long long &oo) -> bool {
-    const long long b = tile0 + tb;
-    if (b >= a.p.total)
-      return false;
-    const long long sl = b / a.p.batch;
-    const long long w = b - sl * a.p.batch;
-    io = sl * a.p.islab + w * a.p.idist;
-    oo = sl * a.p.oslab + w * a.p.odist;
-    return true;
+    io = s_io[tb];
+    oo = s_oo[tb];
+    return io >= 0;
   };
 
   // ---- load ---------------------------------------------------------------
+#pragma unroll 4
   for (int e = tid; e < TB * L; e += kGenThreads) {
     int tb, n;
     if (COL) {
@@ -869,6 +881,7 @@ BF_D void gen_tile(const GenArgs &a, long long tile, unsigned char *smraw) {
 
   // ---- store ----------------------------------------------------------------
   const int lout = a.lout;
+#pragma unroll 4
   for (int e = tid; e < TB * lout; e += kGenThreads) {
     int tb, k;
     if (COL) {

@@ -72,7 +72,9 @@ cudaError_t launch_g(const GenArgs &g, cudaStream_t st) {
   const size_t smem = 2ull * g.TB * g.L * sizeof(cvec<T>);
   if (smem > kGenericSmemLimit)
     return cudaErrorInvalidValue;
-  if (smem > 48 * 1024) {
+  // the tile also holds its transforms' offsets in static shared memory, so
+  // opt in above 48 KiB of total, not of dynamic, shared memory
+  if (smem + kGenStaticSmem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kGenericSmemLimit));
     if (e != cudaSuccess)
@@ -113,9 +115,9 @@ cudaError_t launch_gg(const GenArgs *items, const long long *tile_start, int nit
   auto kern = fft_generic_group_kernel<T, COL, KIND, FWD>;
   if (smem > kGenericSmemLimit)
     return cudaErrorInvalidValue;
-  // the kernel also holds a few bytes of static shared memory, so opt in
-  // above 48 KiB of total, not of dynamic, shared memory
-  if (smem + 256 > 48 * 1024) {
+  // the kernel also holds static shared memory (tile offsets, its task), so
+  // opt in above 48 KiB of total, not of dynamic, shared memory
+  if (smem + kGenStaticSmem + 64 > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(kGenericSmemLimit));
     if (e != cudaSuccess)
