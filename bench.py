@@ -171,6 +171,17 @@ def dist_setup(n_gpus: int):
     return rank, world, local
 
 
+def max_over_ranks(values, pg=None, device="cpu"):
+    """Each value's maximum over all ranks (one all-reduce). Replicas time
+    their own device with CUDA events; the job's time is the slowest rank."""
+    if pg is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def run_reference(args):
     rank, world, local = dist_setup(args.gpus)
     if rank != 0:
@@ -575,10 +586,7 @@ def run_b200(args):
     except Exception as e:  # comparator only
         cufft_ms = f"unavailable: {e}"
 
-    if pg:
-        t = torch.tensor([ms, e2e_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], pg, "cuda")
 
     if rank == 0:
         cpu_ms, cpu_n, cores = time_cpu(host_buf, budget_s=args.cpu_budget, max_steps=8)
