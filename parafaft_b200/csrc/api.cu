@@ -87,6 +87,15 @@ struct HeldCopy {
   size_t bytes = 0;
 };
 
+// A held device-to-device 2D copy (ParaFaFT_R2C::copy_real_to_padded,
+// parafaft_r2c.hpp:804-822): fused into the R2C pass that follows it.
+struct HeldCopy2D {
+  bool active = false;
+  char *dst = nullptr;
+  const char *src = nullptr;
+  size_t dpitch = 0, spitch = 0, width = 0, height = 0;
+};
+
 // An operation recorded while the handle is inside a group.
 struct RecOp {
   enum { PASS = 0, COPY = 1, COPY2D = 2 };
@@ -307,6 +316,7 @@ struct b200fft_handle_s {
   Plan r2c, c2r;
   std::map<int, void *> tables;
   HeldCopy copy;
+  HeldCopy2D pad;
   HeldRun run;
   b200fft_stats stats{};
   std::deque<b200fft_launch_record> log;
@@ -547,6 +557,37 @@ int flush_copy(H *h) {
   return issue_copy(h, h->copy.dst, h->copy.src, h->copy.bytes);
 }
 
+int issue_copy2d(H *h, void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
+                 size_t height) {
+  h->stats.copies_issued++;
+  h->stats.bytes_copied += width * height;
+  b200fft_launch_record r{};
+  r.kind = 3;
+  r.stage = -1;
+  r.family = -1;
+  r.bytes = static_cast<long long>(width * height);
+  if (h->record_only) {
+    push_log(h, r);
+    return B200FFT_SUCCESS;
+  }
+  ProfileScope ps(h);
+  cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height,
+                                    cudaMemcpyDefault, h->stream);
+  push_log(h, r);
+  ps.done();
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaMemcpy2DAsync");
+  return B200FFT_SUCCESS;
+}
+
+int flush_pad(H *h) {
+  if (!h->pad.active)
+    return B200FFT_SUCCESS;
+  h->pad.active = false;
+  const HeldCopy2D c = h->pad;
+  return issue_copy2d(h, c.dst, c.dpitch, c.src, c.spitch, c.width, c.height);
+}
+
 // After a transform consumed [out0, out0+covered) of a held copy, move the
 // parts of the copy it did not cover.
 int finish_fused_copy(H *h, const char *out0, size_t covered) {
@@ -604,11 +645,15 @@ long long pass_bytes(const H *h, const Plan &p, long long total) {
   return total * (p.len * static_cast<long long>(h->rsize) + (p.len / 2 + 1) * cs);
 }
 
+// in_dist >= 0 replaces the input row distance (in the kernel's input units):
+// the R2C pass of a fused pad reads the unpadded source rows.
 int launch_pass(H *h, const Plan &p, int dir, const void *in, void *out,
-                long long slabs, long long slab, bool fused, int stage) {
+                long long slabs, long long slab, bool fused, int stage, long long in_dist = -1) {
   const void *tw = nullptr;
   B2_TRY(get_table(h, p.ch.tlen, &tw));
   PassArgs a = pass_args(p, p.ch.family, in, out, tw, slabs, slab);
+  if (in_dist >= 0)
+    a.idist = in_dist;
   const long long bytes = pass_bytes(h, p, a.total);
   if (h->recording) { // inside a group: the group launches it later
     RecOp op;
@@ -692,6 +737,7 @@ int flush_run(H *h) {
 
 int flush_all(H *h) {
   B2_TRY(flush_run(h));
+  B2_TRY(flush_pad(h));
   return flush_copy(h);
 }
 
@@ -910,6 +956,29 @@ int exec_real(H *h, Plan &p, int kind, void *ptr) {
                                          : "b200fft: execute_c2r_inplace before create_c2r_inplace_plan");
   h->stats.exec_calls++;
   B2_TRY(flush_run(h));
+  if (h->pad.active) {
+    // A held pad copy whose rows are exactly this R2C plan's rows: the pass
+    // reads the unpadded source rows and writes the padded output (every
+    // padded row is overwritten whole, pad lanes included).
+    const HeldCopy2D c = h->pad;
+    const size_t rs = static_cast<size_t>(h->rsize);
+    const size_t unit = p.ch.family == 0 ? 2 * rs : rs; // input units of the kernel
+    const char *src_end = c.src + c.spitch * (c.height - 1) + c.width;
+    const char *dst_end = c.dst + c.dpitch * c.height;
+    const bool match = kind == KIND_R2C && c.dst == ptr && p.stride == 1 &&
+                       c.width == static_cast<size_t>(p.len) * rs &&
+                       c.height == static_cast<size_t>(p.batch) &&
+                       c.dpitch == static_cast<size_t>(p.dist) * rs && c.spitch % unit == 0 &&
+                       reinterpret_cast<uintptr_t>(c.src) % unit == 0 &&
+                       (src_end <= c.dst || dst_end <= c.src);
+    if (match) {
+      h->pad.active = false;
+      h->stats.fused_copies++;
+      return launch_pass(h, p, B200FFT_FORWARD, c.src, ptr, 1, 0, true, -1,
+                         static_cast<long long>(c.spitch / unit));
+    }
+    B2_TRY(flush_pad(h));
+  }
   char *cp = static_cast<char *>(ptr);
   const size_t span = real_span_bytes(h, p);
   bool fused = false;
@@ -1078,6 +1147,7 @@ int b200fft_exec_c2c(b200fft_handle h, int stage, int direction, void *data) {
     return B200FFT_SUCCESS;
   }
   B2_TRY(flush_run(h));
+  B2_TRY(flush_pad(h));
   const long long lead = infer_lead(h, p);
   const size_t slab_bytes = lead > 1 ? static_cast<size_t>(p.len) * p.batch * h->csize()
                                      : c2c_span_bytes(h, p);
@@ -1165,25 +1235,19 @@ int b200fft_memcpy2d(b200fft_handle h, void *dst, size_t dpitch, const void *src
     h->recs.push_back(op);
     return B200FFT_SUCCESS;
   }
-  h->stats.copies_issued++;
-  h->stats.bytes_copied += width * height;
-  b200fft_launch_record r{};
-  r.kind = 3;
-  r.stage = -1;
-  r.family = -1;
-  r.bytes = static_cast<long long>(width * height);
-  if (h->record_only) {
-    push_log(h, r);
+  // Device-to-device copies are held: an R2C pass on the same rows takes
+  // them over (see exec_real); anything else issues them first.
+  if (h->defer && (h->record_only || (is_device_ptr(dst) && is_device_ptr(src)))) {
+    h->pad.active = true;
+    h->pad.dst = static_cast<char *>(dst);
+    h->pad.src = static_cast<const char *>(src);
+    h->pad.dpitch = dpitch;
+    h->pad.spitch = spitch;
+    h->pad.width = width;
+    h->pad.height = height;
     return B200FFT_SUCCESS;
   }
-  ProfileScope ps(h);
-  cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height,
-                                    cudaMemcpyDefault, h->stream);
-  push_log(h, r);
-  ps.done();
-  if (e != cudaSuccess)
-    return cuda_fail(e, "cudaMemcpy2DAsync");
-  return B200FFT_SUCCESS;
+  return issue_copy2d(h, dst, dpitch, src, spitch, width, height);
 }
 
 int b200fft_flush(b200fft_handle h) {

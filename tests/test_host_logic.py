@@ -164,6 +164,30 @@ print(st["kernel_launches"], st["copies_issued"], st["fused_copies"], st["memcpy
 
 
 @pytest.mark.skipif(not _drivers_built(), reason="ParaFaFT drivers not built")
+def test_out_of_place_forward_fuses_the_pad():
+    """ParaFaFT_R2C::forward(real, complex) pads with memcpy2d
+    (parafaft_r2c.hpp:333-339, :804-822) and then runs forward_in_place: the
+    pad is taken over by the R2C pass, so the forward issues 3 launches and
+    no copy; backward(complex, real) keeps its unpad copy."""
+    out = _run_record(r'''
+import ctypes as C
+from parafaft_b200 import native as nv
+f = nv.ParaFaFT("r2c", (64, 64, 64), nv.F32)
+lib = nv.engine()
+cout = C.c_void_p(); nv.check(lib.b200fft_alloc(f.required_size * 4, C.byref(cout)))
+rin = C.c_void_p(); nv.check(lib.b200fft_alloc(64 ** 3 * 4, C.byref(rin)))
+h = f.handle()
+h.reset_stats(); f.forward_oop(rin.value, cout.value); a = h.stats()
+h.reset_stats(); f.backward_oop(cout.value, rin.value); b = h.stats()
+print(a["kernel_launches"], a["copies_issued"], a["fused_copies"], a["memcpy_calls"])
+print(b["kernel_launches"], b["copies_issued"], b["fused_copies"], b["memcpy_calls"])
+''')
+    fwd, bwd = out.strip().splitlines()
+    assert fwd.split() == ["3", "0", "3", "3"]
+    assert bwd.split() == ["3", "1", "2", "3"]
+
+
+@pytest.mark.skipif(not _drivers_built(), reason="ParaFaFT drivers not built")
 def test_no_defer_issues_every_call():
     out = _run_record(r'''
 import os, ctypes as C

@@ -118,6 +118,41 @@ def test_r2c_out_of_place(prec):
     assert O.rel_l2(to_host(rout).reshape(shape) / x.size, x) < tol(prec)
 
 
+@pytest.mark.parametrize("prec", [nv.F64, nv.F32])
+@pytest.mark.parametrize("shape", [(12, 16, 18), (8, 10, 15), (16, 32)])
+def test_fused_pad_matches_unfused(prec, shape, monkeypatch):
+    """The out-of-place forward's pad (memcpy2d) fused into the R2C pass gives
+    bit-for-bit the result of copy-then-transform (B200FFT_NO_DEFER), leaves
+    the real input untouched, and issues no copy for odd D. Odd last axes take
+    the generic kernel (input rows in real units), even ones the specialised
+    one."""
+    _drivers_or_skip()
+    x = O.normal_real(shape, 5).astype(rdtype(prec))
+    f = nv.ParaFaFT("r2c", shape, prec)
+    monkeypatch.setenv("B200FFT_NO_DEFER", "1")
+    g = nv.ParaFaFT("r2c", shape, prec)
+    monkeypatch.delenv("B200FFT_NO_DEFER")
+    outs = []
+    for obj in (f, g):
+        rin = to_dev(x.reshape(-1))
+        cout = to_dev(np.full(obj.required_size, 7.0, dtype=rdtype(prec)))
+        obj.handle().reset_stats()
+        obj.forward_oop(rin, cout)
+        st = obj.handle().stats()
+        np.testing.assert_array_equal(to_host(rin).reshape(shape), x)
+        outs.append((to_host(cout), st))
+    (yf, sf), (yu, su) = outs
+    n = 2 * (x.size // shape[-1]) * (shape[-1] // 2 + 1)
+    np.testing.assert_array_equal(yf[:n], yu[:n])
+    # For even D, forward_in_place first copies the padded output into the
+    # scratch buffer (D-1 odd), so the pad is issued and that copy is fused.
+    assert sf["copies_issued"] == (0 if len(shape) % 2 else 1)
+    assert su["copies_issued"] >= 1
+    nc = shape[-1] // 2 + 1
+    X = yf[:n].view(cdtype(prec)).reshape(shape[:-1] + (nc,))
+    assert O.rel_l2(X, O.r2c_nd(x.astype(np.float64))) < tol(prec)
+
+
 def test_fusion_through_orchestrator():
     """ParaFaFT_R2C<3> forward+backward: 2 x (1 + N0 + 1) backend calls and
     4 exchange copies become 6 launches and no copies."""
