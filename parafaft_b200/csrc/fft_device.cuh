@@ -716,31 +716,33 @@ template <bool COL> BF_D int gidx(int tb, int n, int TB, int L) {
   return COL ? n * TB + tb : tb * L + n;
 }
 
-template <int R, bool FWD, bool COL, typename V>
-BF_D void gen_butterfly(const GenArgs &a, const V *A, V *Bm, const V *tw,
-                        int tb, int j, int k, int Bq, int Ns, int texp) {
+// Generic stage butterflies. `ld(n)` returns point n of the stage input and
+// `st(n, v)` stores point n of its output: shared memory between stages,
+// global memory in the first stage's loads and the last stage's stores.
+template <int R, bool FWD, typename V, class Ld, class St>
+BF_D void gen_butterfly(const GenArgs &a, Ld &&ld, St &&st, const V *tw, int j, int k, int Bq,
+                        int Ns, int texp) {
   V v[R];
 #pragma unroll
   for (int r = 0; r < R; ++r)
-    v[r] = A[gidx<COL>(tb, j + r * Bq, a.TB, a.L)];
+    v[r] = ld(j + r * Bq);
   if (Ns > 1)
     apply_twiddles<R, !FWD>(v, tw, k * texp * a.tscale);
   dft<R, FWD>(v);
   const int base = (j - k) * R + k; // (j/Ns)*Ns*R + k
 #pragma unroll
   for (int r = 0; r < R; ++r)
-    Bm[gidx<COL>(tb, base + r * Ns, a.TB, a.L)] = v[r];
+    st(base + r * Ns, v[r]);
 }
 
 // Prime radix p by direct summation; DFT constants come from the table:
 // exp(-2*pi*i*r*m/p) = tw[((r*m) mod p) * (L/p) * tscale].
-template <bool FWD, bool COL, typename V>
-BF_D void gen_butterfly_prime(const GenArgs &a, const V *A, V *Bm, const V *tw,
-                              int p, int tb, int j, int k, int Bq, int Ns,
-                              int texp) {
+template <bool FWD, typename V, class Ld, class St>
+BF_D void gen_butterfly_prime(const GenArgs &a, Ld &&ld, St &&st, const V *tw, int p, int j,
+                              int k, int Bq, int Ns, int texp) {
   V x[kGenMaxPrime];
   for (int r = 0; r < p; ++r) {
-    V t = A[gidx<COL>(tb, j + r * Bq, a.TB, a.L)];
+    V t = ld(j + r * Bq);
     if (r > 0 && Ns > 1)
       t = cmulw<!FWD>(t, ldtw(tw, r * k * texp * a.tscale));
     x[r] = t;
@@ -756,12 +758,28 @@ BF_D void gen_butterfly_prime(const GenArgs &a, const V *A, V *Bm, const V *tw,
         e -= p;
       acc = cadd(acc, cmulw<!FWD>(x[r], ldtw(tw, e * step)));
     }
-    Bm[gidx<COL>(tb, base + m * Ns, a.TB, a.L)] = acc;
+    st(base + m * Ns, acc);
+  }
+}
+
+template <bool FWD, typename V, class Ld, class St>
+BF_D void gen_radix(const GenArgs &a, int R, Ld &&ld, St &&st, const V *tw, int j, int k, int Bq,
+                    int Ns, int texp) {
+  switch (R) {
+  case 2: gen_butterfly<2, FWD>(a, ld, st, tw, j, k, Bq, Ns, texp); break;
+  case 3: gen_butterfly<3, FWD>(a, ld, st, tw, j, k, Bq, Ns, texp); break;
+  case 4: gen_butterfly<4, FWD>(a, ld, st, tw, j, k, Bq, Ns, texp); break;
+  case 5: gen_butterfly<5, FWD>(a, ld, st, tw, j, k, Bq, Ns, texp); break;
+  case 8: gen_butterfly<8, FWD>(a, ld, st, tw, j, k, Bq, Ns, texp); break;
+  default: gen_butterfly_prime<FWD>(a, ld, st, tw, R, j, k, Bq, Ns, texp); break;
   }
 }
 
 // One tile (a.TB transforms) of a generic pass, run by a whole CTA of
-// kGenThreads threads with 2*TB*L elements of dynamic shared memory.
+// kGenThreads threads with 2*TB*L elements of dynamic shared memory. The
+// first stage reads its points from global memory and (except for R2C, whose
+// Hermitian post-process pairs outputs k and L-k) the last stage writes
+// global memory, so a tile crosses shared memory once per stage boundary.
 template <typename T, bool COL, int KIND, bool FWD>
 BF_D void gen_tile(const GenArgs &a, long long tile, unsigned char *smraw) {
   using V = cvec<T>;
@@ -788,62 +806,84 @@ BF_D void gen_tile(const GenArgs &a, long long tile, unsigned char *smraw) {
     s_oo[tid] = oo;
   }
   __syncthreads();
-  auto offsets = [&](int tb, long long &io, long long &oo) -> bool {
-    io = s_io[tb];
-    oo = s_oo[tb];
-    return io >= 0;
-  };
 
-  // ---- load ---------------------------------------------------------------
-#pragma unroll 4
-  for (int e = tid; e < TB * L; e += kGenThreads) {
-    int tb, n;
-    if (COL) {
-      tb = e & (TB - 1);
-      n = e >> a.logTB;
-    } else {
-      tb = static_cast<int>(fdiv(static_cast<uint32_t>(e), a.Ldiv));
-      n = e - tb * L;
-    }
-    long long io, oo;
+  // Point n of transform tb of the pass input (zero beyond the batch).
+  auto gload = [&](int tb, int n) -> V {
+    const long long io = s_io[tb];
     V val = czero<V>();
-    if (offsets(tb, io, oo)) {
-      const long long is = a.p.istride;
-      if constexpr (KIND == KIND_C2C) {
-        val = reinterpret_cast<const V *>(a.p.in)[io + n * is];
-      } else if constexpr (KIND == KIND_R2C) {
-        const T *x = reinterpret_cast<const T *>(a.p.in) + io;
-        if (a.odd)
-          val = cmake(x[n * is], T(0));
-        else
-          val = cmake(x[(2LL * n) * is], x[(2LL * n + 1) * is]);
-      } else { // C2R
-        const V *X = reinterpret_cast<const V *>(a.p.in) + io;
-        if (a.odd) {
-          const int nh = a.nreal / 2;
-          if (n <= nh) {
-            val = X[n * is];
-            if (n == 0)
-              val.y = T(0);
-          } else {
-            val = cconj(X[(long long)(a.nreal - n) * is]);
-          }
+    if (io < 0)
+      return val;
+    const long long is = a.p.istride;
+    if constexpr (KIND == KIND_C2C) {
+      val = reinterpret_cast<const V *>(a.p.in)[io + n * is];
+    } else if constexpr (KIND == KIND_R2C) {
+      const T *x = reinterpret_cast<const T *>(a.p.in) + io;
+      if (a.odd)
+        val = cmake(x[n * is], T(0));
+      else
+        val = cmake(x[(2LL * n) * is], x[(2LL * n + 1) * is]);
+    } else { // C2R
+      const V *X = reinterpret_cast<const V *>(a.p.in) + io;
+      if (a.odd) {
+        const int nh = a.nreal / 2;
+        if (n <= nh) {
+          val = X[n * is];
+          if (n == 0)
+            val.y = T(0);
         } else {
-          V xa = X[n * is];
-          V xb = X[(long long)(L - n) * is];
-          if (n == 0) {
-            xa.y = T(0);
-            xb.y = T(0);
-          }
-          V ev = cadd(xa, cconj(xb));
-          V ov = cmulw<true>(csub(xa, cconj(xb)), ldtw(tw, n));
-          val = cmake(ev.x - ov.y, ev.y + ov.x);
+          val = cconj(X[(long long)(a.nreal - n) * is]);
         }
+      } else {
+        V xa = X[n * is];
+        V xb = X[(long long)(L - n) * is];
+        if (n == 0) {
+          xa.y = T(0);
+          xb.y = T(0);
+        }
+        V ev = cadd(xa, cconj(xb));
+        V ov = cmulw<true>(csub(xa, cconj(xb)), ldtw(tw, n));
+        val = cmake(ev.x - ov.y, ev.y + ov.x);
       }
     }
-    A[gidx<COL>(tb, n, TB, L)] = val;
+    return val;
+  };
+  // Point k of transform tb of a C2C or C2R pass output.
+  auto gstore = [&](int tb, int k, V z) {
+    const long long oo = s_oo[tb];
+    if (oo < 0)
+      return;
+    const long long os = a.p.ostride;
+    if constexpr (KIND == KIND_C2C) {
+      reinterpret_cast<V *>(a.p.out)[oo + k * os] = z;
+    } else if constexpr (KIND == KIND_C2R) {
+      T *x = reinterpret_cast<T *>(a.p.out) + oo;
+      if (a.odd) {
+        x[k * os] = z.x;
+      } else {
+        x[(2LL * k) * os] = z.x;
+        x[(2LL * k + 1) * os] = z.y;
+      }
+    }
+  };
+
+  const bool direct_in = a.nst > 0;
+  const bool direct_out = a.nst > 0 && KIND != KIND_R2C;
+
+  // ---- load (only for a length without stages) -----------------------------
+  if (!direct_in) {
+    for (int e = tid; e < TB * L; e += kGenThreads) {
+      int tb, n;
+      if (COL) {
+        tb = e & (TB - 1);
+        n = e >> a.logTB;
+      } else {
+        tb = static_cast<int>(fdiv(static_cast<uint32_t>(e), a.Ldiv));
+        n = e - tb * L;
+      }
+      A[gidx<COL>(tb, n, TB, L)] = gload(tb, n);
+    }
+    __syncthreads();
   }
-  __syncthreads();
 
   // ---- stages ---------------------------------------------------------------
   for (int s = 0; s < a.nst; ++s) {
@@ -852,6 +892,8 @@ BF_D void gen_tile(const GenArgs &a, long long tile, unsigned char *smraw) {
     const int Bq = L / R;
     const int texp = L / (Ns * R);
     const int cnt = TB * Bq;
+    const bool first = s == 0;
+    const bool last = s == a.nst - 1 && direct_out;
     for (int q = tid; q < cnt; q += kGenThreads) {
       int tb, j;
       if (COL) {
@@ -862,26 +904,29 @@ BF_D void gen_tile(const GenArgs &a, long long tile, unsigned char *smraw) {
         j = q - tb * Bq;
       }
       const int k = j - static_cast<int>(fdiv(static_cast<uint32_t>(j), a.ns[s])) * Ns;
-      switch (R) {
-      case 2: gen_butterfly<2, FWD, COL>(a, A, Bm, tw, tb, j, k, Bq, Ns, texp); break;
-      case 3: gen_butterfly<3, FWD, COL>(a, A, Bm, tw, tb, j, k, Bq, Ns, texp); break;
-      case 4: gen_butterfly<4, FWD, COL>(a, A, Bm, tw, tb, j, k, Bq, Ns, texp); break;
-      case 5: gen_butterfly<5, FWD, COL>(a, A, Bm, tw, tb, j, k, Bq, Ns, texp); break;
-      case 8: gen_butterfly<8, FWD, COL>(a, A, Bm, tw, tb, j, k, Bq, Ns, texp); break;
-      default:
-        gen_butterfly_prime<FWD, COL>(a, A, Bm, tw, R, tb, j, k, Bq, Ns, texp);
-        break;
-      }
+      auto ld_s = [&](int n) { return A[gidx<COL>(tb, n, TB, L)]; };
+      auto ld_g = [&](int n) { return gload(tb, n); };
+      auto st_s = [&](int n, V v) { Bm[gidx<COL>(tb, n, TB, L)] = v; };
+      auto st_g = [&](int n, V v) { gstore(tb, n, v); };
+      if (first && last)
+        gen_radix<FWD>(a, R, ld_g, st_g, tw, j, k, Bq, Ns, texp);
+      else if (first)
+        gen_radix<FWD>(a, R, ld_g, st_s, tw, j, k, Bq, Ns, texp);
+      else if (last)
+        gen_radix<FWD>(a, R, ld_s, st_g, tw, j, k, Bq, Ns, texp);
+      else
+        gen_radix<FWD>(a, R, ld_s, st_s, tw, j, k, Bq, Ns, texp);
     }
+    if (last)
+      return; // the caller synchronises before the next tile reuses shared memory
     __syncthreads();
     V *t = A;
     A = Bm;
     Bm = t;
   }
 
-  // ---- store ----------------------------------------------------------------
+  // ---- store (R2C, and lengths without stages) ------------------------------
   const int lout = a.lout;
-#pragma unroll 4
   for (int e = tid; e < TB * lout; e += kGenThreads) {
     int tb, k;
     if (COL) {
@@ -891,13 +936,11 @@ BF_D void gen_tile(const GenArgs &a, long long tile, unsigned char *smraw) {
       tb = static_cast<int>(fdiv(static_cast<uint32_t>(e), a.Loutdiv));
       k = e - tb * lout;
     }
-    long long io, oo;
-    if (!offsets(tb, io, oo))
+    const long long oo = s_oo[tb];
+    if (oo < 0)
       continue;
     const long long os = a.p.ostride;
-    if constexpr (KIND == KIND_C2C) {
-      reinterpret_cast<V *>(a.p.out)[oo + k * os] = A[gidx<COL>(tb, k, TB, L)];
-    } else if constexpr (KIND == KIND_R2C) {
+    if constexpr (KIND == KIND_R2C) {
       V *X = reinterpret_cast<V *>(a.p.out) + oo;
       if (a.odd) {
         X[k * os] = A[gidx<COL>(tb, k, TB, L)];
@@ -909,15 +952,8 @@ BF_D void gen_tile(const GenArgs &a, long long tile, unsigned char *smraw) {
         V ov = cmake(T(0.5) * d.y, T(-0.5) * d.x);
         X[k * os] = cadd(ev, cmulw<false>(ov, ldtw(tw, k)));
       }
-    } else { // C2R
-      T *x = reinterpret_cast<T *>(a.p.out) + oo;
-      V z = A[gidx<COL>(tb, k, TB, L)];
-      if (a.odd) {
-        x[k * os] = z.x;
-      } else {
-        x[(2LL * k) * os] = z.x;
-        x[(2LL * k + 1) * os] = z.y;
-      }
+    } else {
+      gstore(tb, k, A[gidx<COL>(tb, k, TB, L)]);
     }
   }
 }
