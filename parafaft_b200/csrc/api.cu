@@ -866,7 +866,7 @@ int autotune(H *h, Plan &p) {
   if (p.ch.family == 0) {
     if (p.ch.col) {
       const int meas[] = {0, 3, 5};
-      const int pat[] = {0, 1, 2, 3, 4, 5, 6};
+      const int pat[] = {0, 1, 2, 3, 4, 5, 6, 7};
       if (rigor >= B200FFT_PLAN_PATIENT)
         for (int v : pat) cands.push_back({0, v});
       else

@@ -153,14 +153,17 @@ constexpr int ce_max(int a, int b) { return a > b ? a : b; }
 //   6 = pipelined column pass: persistent CTAs of 256 threads on half tiles,
 //       the next tile's points loaded into a second register set while the
 //       current one is transformed (two CTAs per SM).
-constexpr int kStaticVariants = 7;
+//   7 = wide column tile on 1024 threads (twice the full tile, half the
+//       points per thread): wide row segments with 32 warps per SM.
+constexpr int kStaticVariants = 8;
 constexpr int kVariantStaged = 4;
 constexpr int kVariantPipelined = 6;
 
 constexpr CfgS cfg_static(int esize, int L, bool col, int variant = 0) {
-  const int NT = (col && (variant >= 3 && variant <= 5)) ? 512 : 256;
+  const int NT = (col && variant == 7) ? 1024
+                 : (col && (variant >= 3 && variant <= 5)) ? 512 : 256;
   const int base = esize == 8 ? 8192 : 4096;
-  const int target = col ? (variant == 3 ? 2 * base
+  const int target = col ? ((variant == 3 || variant == 7) ? 2 * base
                                          : (variant == 4 || variant == 5)
                                                ? base
                                                : variant == 6 ? base / 2 : (base >> variant))

@@ -126,6 +126,11 @@ cudaError_t launch_static_var(int var, const PassArgs &a, cudaStream_t st) {
       return launch_static_one<T, L, COL, FWD, KIND, 5>(a, st);
     else
       return launch_static_one<T, L, COL, FWD, KIND, 0>(a, st);
+  case 7:
+    if constexpr (COL)
+      return launch_static_one<T, L, COL, FWD, KIND, 7>(a, st);
+    else
+      return launch_static_one<T, L, COL, FWD, KIND, 0>(a, st);
   default: return launch_static_one<T, L, COL, FWD, KIND, 0>(a, st);
   }
 }
