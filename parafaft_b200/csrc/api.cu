@@ -63,7 +63,8 @@ bool env_flag(const char *name) {
 
 // Kernel choice of a plan.
 struct Choice {
-  int family = 0; // 0 static, 1 generic, 2 split-precision tensor core
+  int family = 0; // 0 static, 1 generic, 2 split-precision tensor core (mma.sync),
+                  // 3 split-precision tensor core on tcgen05
   bool col = false;
   int L = 0;      // complex points of the stage loop
   int tlen = 0;   // twiddle table length
@@ -197,6 +198,11 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
     ch.variant = 0;
     ch.TB = ch.col ? 16 : 4;
     ch.NT = ch.col ? (L == 1024 ? 512 : 256) : 128;
+    if (!ch.col && L == 256 && env_flag("B200FFT_TC5")) { // tcgen05 rows
+      ch.family = 3;
+      ch.TB = 8;
+      ch.NT = 128;
+    }
     *out = ch;
     return B200FFT_SUCCESS;
   }
@@ -266,7 +272,7 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
 std::string describe_choice(const Choice &ch, int kind) {
   char buf[256];
   std::string rad;
-  if (ch.family == 2) {
+  if (ch.family >= 2) {
     rad = (ch.L > 256 ? std::to_string(ch.L / 256) + "x" : std::string()) + "16x16";
   } else if (ch.family == 0) {
     int m = ch.L;
@@ -284,7 +290,11 @@ std::string describe_choice(const Choice &ch, int kind) {
     rad = "1";
   const char *kn = kind == KIND_C2C ? "c2c" : (kind == KIND_R2C ? "r2c" : "c2r");
   std::snprintf(buf, sizeof(buf), "%s %s L=%d %s tb=%d nt=%d radices=%s var=%d",
-                ch.family == 0 ? "static" : (ch.family == 2 ? "split-tc" : "generic"), kn, ch.L,
+                ch.family == 0   ? "static"
+                : ch.family == 2 ? "split-tc"
+                : ch.family == 3 ? "split-tc5"
+                                 : "generic",
+                kn, ch.L,
                 ch.col ? "col" : "row", ch.TB, ch.NT, rad.c_str(), ch.variant);
   return buf;
 }
@@ -309,6 +319,7 @@ struct b200fft_handle_s {
   bool defer = true;
   bool force_generic = false;
   bool split_tc = false; // split-precision tensor-core kernels where they exist
+  bool used_tc5 = false; // launched a tcgen05 kernel (check its fault word at sync)
   int device = -1;
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
@@ -711,6 +722,9 @@ cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
               : launch_static_c2r_f32(p.ch.L, p.ch.variant, a, h->stream);
   } else if (p.ch.family == 2) {
     e = launch_tc_c2c_f32(p.ch.L, p.ch.col, fwd, a, h->stream);
+  } else if (p.ch.family == 3) {
+    h->used_tc5 = true;
+    e = launch_tc5_row256_f32(fwd, a, h->stream);
   } else {
     GenArgs g = p.ch.gen;
     g.p = a;
@@ -939,7 +953,7 @@ int make_plan(H *h, Plan *dst, int kind, int length, size_t batch,
   *dst = p; // visible to infer_lead while tuning
   // The split-precision kernels are a precision choice, not a tuning
   // candidate: plans that use them are not timed against the plain ones.
-  if (h->plan_flag >= B200FFT_PLAN_MEASURE && !h->force_generic && p.ch.family != 2 &&
+  if (h->plan_flag >= B200FFT_PLAN_MEASURE && !h->force_generic && p.ch.family < 2 &&
       std::getenv("B200FFT_VARIANT") == nullptr) {
     B2_TRY(autotune(h, p));
     *dst = p;
@@ -1263,6 +1277,16 @@ int b200fft_sync(b200fft_handle h) {
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess)
     return cuda_fail(e, "cudaStreamSynchronize");
+  if (h->used_tc5) {
+    unsigned fault = 0;
+    e = tc5_take_fault(&fault);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "tensor-core fault word");
+    if (fault)
+      return fail(B200FFT_ERR_DEVICE_STATUS,
+                  "b200fft: a tensor-core kernel gave up waiting for its products "
+                  "(results of that launch are invalid)");
+  }
   return B200FFT_SUCCESS;
 }
 

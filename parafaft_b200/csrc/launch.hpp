@@ -28,6 +28,12 @@ size_t static_smem_bytes(int esize_complex, int L, bool col, int var);
 cudaError_t launch_tc_c2c_f32(int L, bool col, bool fwd, const PassArgs &a, cudaStream_t st);
 size_t tc_smem_bytes(int L, bool col);
 constexpr bool tc_length_ok(int L) { return L == 256 || L == 512 || L == 1024; }
+// The same on the fifth-generation tensor cores (tcgen05, TMEM accumulators):
+// FP32 C2C rows of length 256.
+cudaError_t launch_tc5_row256_f32(bool fwd, const PassArgs &a, cudaStream_t st);
+// The tcgen05 kernels' device fault word (a bounded wait that ran out),
+// returned and cleared; call after the launches' stream is synchronised.
+cudaError_t tc5_take_fault(unsigned *fault);
 
 // Family G: runtime-generic kernels.
 cudaError_t launch_generic(bool f64, int kind, bool col, bool fwd,
