@@ -343,7 +343,7 @@ def gaussian_random_field(shape, seed: int, slope: float = -3.0) -> np.ndarray:
     nz = k > 0
     amp[nz] = k[nz] ** (slope / 2.0)
     noise = rng.standard_normal(k.shape) + 1j * rng.standard_normal(k.shape)
-    field = np.fft.irfftn(noise * amp, s=shape)
+    field = np.fft.irfftn(noise * amp, s=shape, axes=tuple(range(len(shape))))
     return field
 
 

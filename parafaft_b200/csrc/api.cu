@@ -198,7 +198,10 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
     ch.variant = 0;
     ch.TB = ch.col ? 16 : 4;
     ch.NT = ch.col ? (L == 1024 ? 512 : 256) : 128;
-    if (!ch.col && L == 256 && env_flag("B200FFT_TC5")) { // tcgen05 rows
+    // 256-point rows run on the tcgen05 kernel (faster than the mma.sync one);
+    // B200FFT_TC_FORM=mma keeps them on mma.sync
+    const char *form = std::getenv("B200FFT_TC_FORM");
+    if (!ch.col && L == 256 && !(form != nullptr && std::string(form) == "mma")) {
       ch.family = 3;
       ch.TB = 8;
       ch.NT = 128;

@@ -88,15 +88,17 @@ BF_D void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "
 BF_D void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // Wait for phase `parity` of the barrier, at most about a second of clock.
+// One thread polls (suspended up to 1 us per try); the others wait at the
+// CTA barrier that follows, which costs them no issue slots.
 BF_D bool mbar_wait(uint32_t mbar, uint32_t parity) {
   const long long t0 = clock64();
   for (;;) {
     uint32_t done;
     asm volatile("{\n\t.reg .pred P1;\n\t"
-                 "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
                  "selp.b32 %0, 1, 0, P1;\n\t}\n"
                  : "=r"(done)
-                 : "r"(mbar), "r"(parity)
+                 : "r"(mbar), "r"(parity), "r"(1000u)
                  : "memory");
     if (done)
       return true;
@@ -170,10 +172,13 @@ BF_D void issue_step(uint32_t tmem, const unsigned char *A, const unsigned char 
   umma(acc_a, ad(0), bd(0), id, 0); // hi re * hi
 }
 
-// Six CTAs per SM (85 registers, 20 KB of shared memory, 384 of 512 TMEM
+// Eight CTAs per SM (64 registers, 20 KB of shared memory, all 512 TMEM
 // columns): the CTAs' load / product / store chains overlap one another.
 template <bool FWD>
-__global__ void __launch_bounds__(kTc5Threads, 6) fft_tc5_row256_kernel(PassArgs a) {
+// stall != 0 (a host-side test switch) issues no products and waits on a
+// barrier phase that nothing completes, so the bounded wait runs out and the
+// fault path is exercised without any GPU fault.
+__global__ void __launch_bounds__(kTc5Threads, 8) fft_tc5_row256_kernel(PassArgs a, int stall) {
   // step 2's operand reuses step 1's: the step-1 products have completed
   // (their barrier phase observed) before it is written
   __shared__ __align__(128) unsigned char sA1[4 * kRegA];
@@ -265,11 +270,13 @@ __global__ void __launch_bounds__(kTc5Threads, 6) fft_tc5_row256_kernel(PassArgs
     __syncthreads();
     fence_after();
     if (tid == 0) {
-      issue_step(tmem, sA1, sB, false);
-      umma_commit(mb);
+      if (!stall) {
+        issue_step(tmem, sA1, sB, false);
+        umma_commit(mb);
+      }
+      if (!mbar_wait(mb, phase))
+        abort_s = 1;
     }
-    if (!mbar_wait(mb, phase))
-      abort_s = 1;
     phase ^= 1;
     fence_after();
     __syncthreads();
@@ -320,9 +327,9 @@ __global__ void __launch_bounds__(kTc5Threads, 6) fft_tc5_row256_kernel(PassArgs
     if (tid == 0) {
       issue_step(tmem, sA2, sB, true);
       umma_commit(mb);
+      if (!mbar_wait(mb, phase))
+        abort_s = 1;
     }
-    if (!mbar_wait(mb, phase))
-      abort_s = 1;
     phase ^= 1;
     fence_after();
     __syncthreads();
@@ -387,10 +394,12 @@ cudaError_t launch_tc5_row256_f32(bool fwd, const PassArgs &a, cudaStream_t st) 
     sms = 148;
   const long long slots = static_cast<long long>(sms) * per_sm[dev];
   const long long grid = ntiles < slots ? ntiles : slots;
+  const char *sv = std::getenv("B200FFT_TC5_STALL_TEST");
+  const int stall = (sv != nullptr && sv[0] == '1') ? 1 : 0;
   if (fwd)
-    fft_tc5_row256_kernel<true><<<static_cast<unsigned>(grid), kTc5Threads, 0, st>>>(a);
+    fft_tc5_row256_kernel<true><<<static_cast<unsigned>(grid), kTc5Threads, 0, st>>>(a, stall);
   else
-    fft_tc5_row256_kernel<false><<<static_cast<unsigned>(grid), kTc5Threads, 0, st>>>(a);
+    fft_tc5_row256_kernel<false><<<static_cast<unsigned>(grid), kTc5Threads, 0, st>>>(a, stall);
   return cudaGetLastError();
 }
 

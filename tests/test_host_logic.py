@@ -85,6 +85,8 @@ def test_split_tc_selection():
     assert d.plan_describe(nv.KIND_C2C, 0).startswith("static c2c L=1024")
     h.plan_c2c(1, 1024, 64, 64, 1)  # a 1024-point column tile uses 16 warps
     assert h.plan_describe(nv.KIND_C2C, 1).startswith("split-tc c2c L=1024 col tb=16 nt=512")
+    h.plan_c2c(2, 256, 100, 1, 256)  # 256-point rows: the tcgen05 kernel
+    assert h.plan_describe(nv.KIND_C2C, 2).startswith("split-tc5 c2c L=256 row tb=8 nt=128")
 
 
 def test_supported_lengths():

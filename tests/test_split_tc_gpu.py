@@ -174,3 +174,39 @@ def test_roundtrip_through_orchestrator(monkeypatch, kind, shape):
     f.backward(d)
     back = to_host(d)[:x.size].reshape(shape) / x.size
     assert O.rel_l2(back, x) < REL_F32
+
+
+@pytest.mark.parametrize("direction", [nv.FORWARD, nv.BACKWARD])
+def test_rows_256_mma_sync_form(direction, monkeypatch):
+    """256-point rows run on the tcgen05 kernel by default; the mma.sync form
+    stays available (B200FFT_TC_FORM=mma) and meets the same bound."""
+    monkeypatch.setenv("B200FFT_TC_FORM", "mma")
+    x = O.normal_complex(256 * 37, 3)
+    y, desc = _run(x, 256, 37, 1, 256, direction, True)
+    assert desc.startswith("split-tc c2c L=256 row"), desc
+    ref = O.c2c_batch(x, 256, 37, 1, 256, -1 if direction == nv.FORWARD else +1)
+    assert O.rel_l2(y, ref) < REL_F32
+
+
+def test_tcgen05_wait_limit_reports_device_status(monkeypatch):
+    """The tcgen05 kernel bounds every wait for its products. With the test
+    switch set, thread 0 issues nothing and waits on a barrier phase that never
+    completes: the wait runs out (about a second), the CTAs free their tensor
+    memory and return, and b200fft_sync reports B200FFT_ERR_DEVICE_STATUS. The
+    context stays usable: the next transform is correct."""
+    x = O.normal_complex(256 * 16, 4)
+    h = nv.Handle(nv.F32, 1, flags=nv.FLAG_SPLIT_TC)
+    h.plan_c2c(0, 256, 16, 1, 256)
+    assert h.plan_describe(nv.KIND_C2C, 0).startswith("split-tc5")
+    d = to_dev(x.astype(np.complex64))
+    monkeypatch.setenv("B200FFT_TC5_STALL_TEST", "1")
+    h.exec_c2c(0, nv.FORWARD, d)
+    with pytest.raises(nv.B200FFTError) as e:
+        h.sync()
+    assert e.value.code == -7
+    monkeypatch.delenv("B200FFT_TC5_STALL_TEST")
+    d = to_dev(x.astype(np.complex64))
+    h.exec_c2c(0, nv.FORWARD, d)
+    h.sync()
+    ref = O.c2c_batch(x, 256, 16, 1, 256, -1)
+    assert O.rel_l2(to_host(d), ref) < REL_F32
