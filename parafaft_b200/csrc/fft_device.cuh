@@ -365,7 +365,6 @@ struct KS {
         // lane g holds Z[g + P*m] in v[(m % BP)*R + m / BP]
         constexpr int NM = L / P;
         constexpr int BP = B / P;
-        const V wg = ldtw(c.tw, c.g);
         const int src = (P - c.g) & (P - 1);
 #pragma unroll
         for (int m = 0; m < NM; ++m) {
@@ -376,7 +375,7 @@ struct KS {
             zb = v[(m2 % BP) * R + m2 / BP];
           }
           const V za = v[(m % BP) * R + m / BP];
-          const V w = m == 0 ? wg : cmulw<false>(wg, ldtw(c.tw, P * m));
+          const V w = ldtw(c.tw, c.g + P * m); // coalesced table read
           if (c.act)
             c.gout[(long long)(c.g + P * m) * c.ost] = r2c_from_pair(za, zb, w);
         }
@@ -488,7 +487,6 @@ struct KS {
       for (int m = 0; m < NM; ++m)
         x[m] = c.act ? c.gin[(long long)(c.g + P * m) * c.ist] : czero<V>();
       const V xl = (c.act && c.g == 0) ? c.gin[(long long)L * c.ist] : czero<V>();
-      const V wg = ldtw(c.tw, c.g);
       const int src = (P - c.g) & (P - 1);
 #pragma unroll
       for (int m = 0; m < NM; ++m) {
@@ -501,7 +499,7 @@ struct KS {
             xb.y = T(0);
           }
         }
-        const V w = m == 0 ? wg : cmulw<false>(wg, ldtw(c.tw, P * m));
+        const V w = ldtw(c.tw, c.g + P * m); // coalesced table read
         v[(m % BP) * R + m / BP] = c2r_from_pair(xa, xb, w);
       }
       run<0>(c, v);
