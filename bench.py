@@ -445,6 +445,53 @@ def run_uneven(args):
     return 0
 
 
+def measure_split_tc(args, pinned, x_real, dev, stream, plain_ms):
+    """The 512^3 R2C forward+backward with B200FFT_SPLIT_TC=1 (its 512-point
+    column passes on the split-precision tensor-core kernels): device ms per
+    step, forward rel-L2 against the FP64 reference, and plain / split."""
+    import torch
+    from parafaft_b200 import native as nv
+    from oracle import oracle as O
+    old = os.environ.get("B200FFT_SPLIT_TC")
+    os.environ["B200FFT_SPLIT_TC"] = "1"
+    try:
+        f = nv.ParaFaFT("r2c", SHAPE, nv.F32)
+    finally:
+        if old is None:
+            os.environ.pop("B200FFT_SPLIT_TC")
+        else:
+            os.environ["B200FFT_SPLIT_TC"] = old
+    try:
+        h = f.handle()
+        h.set_stream(stream.cuda_stream)
+        kinds = sorted({h.plan_describe(nv.KIND_C2C, s).split()[0] for s in (1, 2)})
+        with torch.cuda.stream(stream):
+            dev.copy_(pinned, non_blocking=True)
+        f.forward(dev)
+        X = dev.cpu().numpy().view(np.complex64).reshape(512, 512, 257)
+        rel = O.rel_l2(X, O.r2c_nd(x_real.astype(np.float64), impl="scipy"))
+        del X
+        with torch.cuda.stream(stream):
+            dev.copy_(pinned, non_blocking=True)
+        for _ in range(args.warmup):
+            f.forward(dev)
+            f.backward(dev)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            f.forward(dev)
+            f.backward(dev)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        return {"ms": round(ms, 4), "rel_l2_fwd_vs_fp64": rel, "column_kernels": kinds,
+                "speedup_vs_plain": round(plain_ms / ms, 3)}
+    finally:
+        f.close()
+
+
 def run_b200(args):
     import torch
     from parafaft_b200 import native as nv
@@ -560,6 +607,10 @@ def run_b200(args):
     torch.cuda.synchronize()
     e2e_ms = e2.elapsed_time(e3) / args.steps
 
+    # ---- the split-precision tensor-core form of the same workload: the
+    #      column passes (512-point C2C) on the tensor cores, FP16 hi+lo
+    split = measure_split_tc(args, pinned, x_real, dev, stream, ms)
+
     # ---- the reference's cuFFT backend on the same GPU, same orchestrator
     cufft_ms = None
     try:
@@ -610,6 +661,7 @@ def run_b200(args):
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes},
             "cufft_backend_ms": cufft_ms if isinstance(cufft_ms, str) else round(cufft_ms, 4),
+            "split_tc": split,
             "gpu_launches": int(launches),
             "clocks": clk,
             "cpu_baseline": {"value": round(cpu_ms, 1), "unit": "ms", "cores": cores, "kind": "port",
