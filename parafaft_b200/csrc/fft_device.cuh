@@ -976,32 +976,42 @@ __global__ void __launch_bounds__(kGenThreads)
                              const long long *__restrict__ tile_start, int nitems,
                              unsigned long long *queue) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ long long task_s;
-  __shared__ int item_s;
+  __shared__ long long task_s[2];
+  __shared__ int item_s[2];
   const long long ntasks = tile_start[nitems];
-  for (;;) {
-    if (threadIdx.x == 0) {
-      const long long t = static_cast<long long>(atomicAdd(queue, 1ull));
-      int lo = 0, hi = nitems - 1;
-      if (t < ntasks) {
-        while (lo < hi) { // last item whose first tile is <= t
-          const int mid = (lo + hi + 1) >> 1;
-          if (tile_start[mid] <= t)
-            lo = mid;
-          else
-            hi = mid - 1;
-        }
+  // Map a claimed tile number to its item (binary search on tile_start).
+  auto resolve = [&](long long t, int slot) {
+    int lo = 0, hi = nitems - 1;
+    if (t < ntasks) {
+      while (lo < hi) { // last item whose first tile is <= t
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile_start[mid] <= t)
+          lo = mid;
+        else
+          hi = mid - 1;
       }
-      task_s = t;
-      item_s = lo;
     }
-    __syncthreads();
-    const long long t = task_s;
-    const int i = item_s;
+    task_s[slot] = t;
+    item_s[slot] = lo;
+  };
+  if (threadIdx.x == 0)
+    resolve(static_cast<long long>(atomicAdd(queue, 1ull)), 0);
+  __syncthreads();
+  for (int it = 0;; ++it) {
+    const int cur = it & 1;
+    const long long t = task_s[cur];
+    const int i = item_s[cur];
     if (t >= ntasks)
       return;
+    // The next claim is issued now and resolved after this tile, so the
+    // atomic's round trip overlaps the tile's work.
+    unsigned long long next = 0;
+    if (threadIdx.x == 0)
+      next = atomicAdd(queue, 1ull);
     gen_tile<T, COL, KIND, FWD>(items[i], t - tile_start[i], smraw);
-    __syncthreads(); // shared memory and task_s are reused by the next tile
+    if (threadIdx.x == 0)
+      resolve(static_cast<long long>(next), cur ^ 1);
+    __syncthreads(); // shared memory and the next task are ready
   }
 }
 
