@@ -219,6 +219,8 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
         var = v[0] - '0';
     if (variant >= 0 && variant < kStaticVariants)
       var = variant;
+    if (!is_pow2(L))
+      var = 0; // mixed-radix lengths have the full tile only
     const CfgS c = cfg_static(csize, L, ch.col, var);
     ch.variant = var;
     ch.family = 0;
@@ -283,6 +285,8 @@ std::string describe_choice(const Choice &ch, int kind) {
     while (m % 8 == 0 && m > 1) { r.push_back(8); m /= 8; }
     if (m % 4 == 0) { r.push_back(4); m /= 4; }
     if (m % 2 == 0) { r.push_back(2); m /= 2; }
+    while (m % 5 == 0) { r.push_back(5); m /= 5; }
+    while (m % 3 == 0) { r.push_back(3); m /= 3; }
     for (size_t i = 0; i < r.size(); ++i)
       rad += (i ? "x" : "") + std::to_string(r[i]);
   } else {

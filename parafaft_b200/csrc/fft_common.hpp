@@ -159,7 +159,27 @@ constexpr int kStaticVariants = 8;
 constexpr int kVariantStaged = 4;
 constexpr int kVariantPipelined = 6;
 
+constexpr bool is_pow2(long long x) { return x > 0 && (x & (x - 1)) == 0; }
+constexpr int floor_pow2(int x) {
+  int p = 1;
+  while (p * 2 <= x)
+    p *= 2;
+  return p;
+}
+
 constexpr CfgS cfg_static(int esize, int L, bool col, int variant = 0) {
+  if (!is_pow2(L)) {
+    // Mixed-radix lengths (factors 8, 4, 2, 5, 3): the full tile only, with
+    // power-of-two tiles and thread counts per transform.
+    const int NT = 256;
+    const int base = esize == 8 ? 8192 : 4096;
+    if (col) {
+      const int TB = ce_min(NT, floor_pow2(ce_max(1, base / L)));
+      return CfgS{NT, TB, NT / TB, (TB * L + NT - 1) / NT};
+    }
+    const int P = ce_min(NT, floor_pow2(ce_max(1, L / 8)));
+    return CfgS{NT, NT / P, P, (L + P - 1) / P};
+  }
   const int NT = (col && variant == 7) ? 1024
                  : (col && (variant >= 3 && variant <= 5)) ? 512 : 256;
   const int base = esize == 8 ? 8192 : 4096;
@@ -195,10 +215,15 @@ constexpr CfgS cfg_static(int esize, int L, bool col, int variant = 0) {
   return CfgS{NT, TB, P, E};
 }
 
-constexpr bool is_pow2(long long x) { return x > 0 && (x & (x - 1)) == 0; }
-
-// Lengths with a specialised kernel (complex points of the stage loop).
+// Lengths with a specialised kernel (complex points of the stage loop):
+// powers of two up to 4096, and the mixed-radix lengths below (the sides of
+// common non-power-of-two grids and their R2C halves).
 constexpr int kStaticMaxL = 4096;
-constexpr bool static_length_ok(int L) { return L >= 2 && L <= kStaticMaxL && is_pow2(L); }
+constexpr bool static_pow2_ok(int L) { return L >= 2 && L <= kStaticMaxL && is_pow2(L); }
+constexpr bool static_mixed_ok(int L) {
+  return L == 24 || L == 30 || L == 40 || L == 48 || L == 60 || L == 80 || L == 96 ||
+         L == 120 || L == 160 || L == 192 || L == 384 || L == 768;
+}
+constexpr bool static_length_ok(int L) { return static_pow2_ok(L) || static_mixed_ok(L); }
 
 } // namespace b200fft

@@ -352,7 +352,10 @@ struct KS {
         const int j = c.g + P * i;
         if (FULL || j < B) {
           const int k = j % Ns;
-          apply_twiddles_pyr<R, !FWD>(&v[i * R], c.tw + (2 * TM - 2 * Ns * R), Ns * R, k);
+          if constexpr ((L & (L - 1)) == 0) // pyramid: level Ns*R at offset 2TM - 2Ns*R
+            apply_twiddles_pyr<R, !FWD>(&v[i * R], c.tw + (2 * TM - 2 * Ns * R), Ns * R, k);
+          else // flat table of TM entries: w^(r k) at r * k * TM / (Ns R)
+            apply_twiddles<R, !FWD>(&v[i * R], c.tw, k * (TM / (Ns * R)));
         }
       }
     }

@@ -107,6 +107,8 @@ cudaError_t launch_static_pipelined(const PassArgs &a, cudaStream_t st) {
 
 template <typename T, int L, bool COL, bool FWD, int KIND>
 cudaError_t launch_static_var(int var, const PassArgs &a, cudaStream_t st) {
+  if constexpr (!is_pow2(L)) // mixed-radix lengths have the full tile only
+    return launch_static_one<T, L, COL, FWD, KIND, 0>(a, st);
   if constexpr (COL && KIND == KIND_C2C) {
     if (var == kVariantStaged)
       return launch_static_staged<T, L, FWD>(a, st);
@@ -144,6 +146,9 @@ cudaError_t launch_static_switch(int L, int var, const PassArgs &a, cudaStream_t
     B2_FS_CASE(2) B2_FS_CASE(4) B2_FS_CASE(8) B2_FS_CASE(16) B2_FS_CASE(32)
     B2_FS_CASE(64) B2_FS_CASE(128) B2_FS_CASE(256) B2_FS_CASE(512)
     B2_FS_CASE(1024) B2_FS_CASE(2048)
+    B2_FS_CASE(24) B2_FS_CASE(30) B2_FS_CASE(40) B2_FS_CASE(48) B2_FS_CASE(60)
+    B2_FS_CASE(80) B2_FS_CASE(96) B2_FS_CASE(120) B2_FS_CASE(160) B2_FS_CASE(192)
+    B2_FS_CASE(384) B2_FS_CASE(768)
   case 4096:
     if constexpr (KIND == KIND_C2C)
       return launch_static_var<T, 4096, COL, FWD, KIND>(var, a, st);

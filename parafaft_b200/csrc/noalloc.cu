@@ -98,7 +98,7 @@ extern "C" int b200fft_c2c_noalloc(int precision, int direction, int length, siz
   if (in == nullptr || out == nullptr || batch < 1 || stride < 1 || dist < 1)
     return fail(B200FFT_ERR_INVALID_ARG,
                 "b200fft_c2c_noalloc: null data pointer or batch/stride/dist below 1");
-  if (length > kNoAllocMaxLength || !static_length_ok(length))
+  if (length > kNoAllocMaxLength || !static_pow2_ok(length))
     return fail(B200FFT_ERR_UNSUPPORTED,
                 "b200fft_c2c_noalloc: length " + std::to_string(length) +
                     " is not a power of two in [2, " + std::to_string(kNoAllocMaxLength) +

@@ -255,3 +255,47 @@ def test_tile_variants(prec, variant, length, monkeypatch):
     for stride, dist in ((batch, 1), (1, length)):
         y, ref, h = _c2c_case(prec, length, batch, stride, dist, nv.BACKWARD, seed=variant)
         assert O.rel_l2(y, ref) < tol(prec), (variant, length, stride)
+
+
+MIXED_STATIC = [24, 30, 40, 48, 60, 80, 96, 120, 160, 192, 384, 768]
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("length", MIXED_STATIC)
+def test_mixed_radix_specialised_kernels(prec, length):
+    """Lengths of factors 8, 4, 2, 5, 3 with a specialised kernel (flat FP64
+    twiddle table, power-of-two tiles): rows, columns and strided rows against
+    the oracle, and the same plans on the generic kernel."""
+    batch = 37
+    assert nv.describe(prec, nv.KIND_C2C, length).startswith("static")
+    for stride, dist in ((1, length), (batch, 1), (3, 3 * length + 1)):
+        for direction in (nv.FORWARD, nv.BACKWARD):
+            y, ref, _ = _c2c_case(prec, length, batch, stride, dist, direction, seed=length)
+            assert O.rel_l2(y, ref) < tol(prec), (length, stride, dist, direction)
+    g, ref, _ = _c2c_case(prec, length, batch, batch, 1, nv.FORWARD, flags=nv.FLAG_GENERIC_ONLY)
+    assert O.rel_l2(g, ref) < tol(prec)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("n", [48, 60, 80, 96, 120, 160, 384, 768, 1536])
+def test_mixed_radix_r2c_c2r_specialised(prec, n):
+    """R2C / C2R of even non-power-of-two lengths on the specialised kernels
+    (half length in the mixed-radix set) against the oracle, padded rows."""
+    batch = 21
+    dist = 2 * (n // 2 + 1)
+    assert nv.describe(prec, nv.KIND_R2C, n).startswith("static")
+    x = O.normal_real((batch, n), n)
+    buf = np.zeros(batch * dist, dtype=rdtype(prec))
+    buf.reshape(batch, dist)[:, :n] = x
+    h = nv.Handle(prec, 1)
+    h.plan_r2c(n, batch, 1, dist)
+    h.plan_c2r(n, batch, 1, dist)
+    d = to_dev(buf)
+    h.exec_r2c(d)
+    h.sync()
+    X = to_host(d).view(cdtype(prec)).reshape(batch, dist // 2)
+    assert O.rel_l2(X, np.fft.rfft(x, axis=1)) < tol(prec)
+    h.exec_c2r(d)
+    h.sync()
+    back = to_host(d).reshape(batch, dist)[:, :n] / n
+    assert O.rel_l2(back, x) < tol(prec)

@@ -55,9 +55,11 @@ def test_argument_validation():
 
 
 @pytest.mark.parametrize("kind,n,expect", [
-    (nv.KIND_C2C, 512, "static c2c L=512"), (nv.KIND_C2C, 60, "generic c2c L=60"),
+    (nv.KIND_C2C, 512, "static c2c L=512"), (nv.KIND_C2C, 60, "static c2c L=60"),
+    (nv.KIND_C2C, 100, "generic c2c L=100"), (nv.KIND_C2C, 120, "static c2c L=120 row tb=32 nt=256 radices=8x5x3"),
     (nv.KIND_R2C, 512, "static r2c L=256"), (nv.KIND_R2C, 63, "generic r2c L=63"),
-    (nv.KIND_C2R, 160, "generic c2r L=80"), (nv.KIND_C2C, 4096, "static c2c L=4096"),
+    (nv.KIND_C2R, 160, "static c2r L=80"), (nv.KIND_C2R, 200, "generic c2r L=100"),
+    (nv.KIND_C2C, 4096, "static c2c L=4096"), (nv.KIND_C2C, 768, "static c2c L=768"),
 ])
 def test_kernel_selection(kind, n, expect):
     assert nv.describe(nv.F32, kind, n).startswith(expect)
