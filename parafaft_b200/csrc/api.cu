@@ -362,14 +362,18 @@ struct b200fft_handle_s {
 namespace {
 
 struct GroupStep {
-  enum { PASSES = 0, COPY = 1, COPY2D = 2 };
+  enum { PASSES = 0, COPY = 1, COPY2D = 2, STATIC = 3 };
   int type = PASSES;
-  // grouped generic pass
+  // grouped pass: generic kernel (PASSES, items) or specialised kernel of
+  // length L (STATIC, sitems)
   bool f64 = false, col = false, fwd = true;
   int kind = KIND_C2C;
+  int L = 0;
   std::vector<GenArgs> items;
+  std::vector<PassArgs> sitems;
   std::vector<long long> tile_start;
   GenArgs *d_items = nullptr;
+  PassArgs *d_sitems = nullptr;
   long long *d_tile_start = nullptr;
   size_t smem = 0;
   int grid = 0;
@@ -1505,6 +1509,8 @@ void group_free_schedule(G *g) {
     for (GroupStep &s : g->steps) {
       if (s.d_items)
         cudaFree(s.d_items);
+      if (s.d_sitems)
+        cudaFree(s.d_sitems);
       if (s.d_tile_start)
         cudaFree(s.d_tile_start);
     }
@@ -1533,7 +1539,7 @@ int group_build(G *g) {
   for (H *h : g->handles)
     depth = std::max(depth, h->recs.size());
   for (size_t d = 0; d < depth; ++d) {
-    std::map<int, size_t> bucket; // (f64, kind, col, fwd) -> step index
+    std::map<long long, size_t> bucket; // (static, L, f64, kind, col, fwd) -> step index
     for (H *h : g->handles) {
       if (d >= h->recs.size())
         continue;
@@ -1546,6 +1552,43 @@ int group_build(G *g) {
         continue;
       }
       const Plan &p = op.plan;
+      const bool f64s = h->prec == B200FFT_F64;
+      const bool fwds = op.dir == B200FFT_FORWARD;
+      // A pass with a specialised kernel joins the grouped launch of that
+      // kernel (same length, layout, kind and direction), full tile.
+      Choice sc;
+      if (!h->force_generic &&
+          choose_kernel(h->prec, p.kind, p.len, p.batch, p.stride, p.dist, false, &sc, 0) ==
+              B200FFT_SUCCESS &&
+          sc.family == 0) {
+        const long long key = (1ll << 40) | (static_cast<long long>(sc.L) << 8) |
+                              (f64s ? 1 : 0) | (p.kind << 1) | ((sc.col ? 1 : 0) << 3) |
+                              ((fwds ? 1 : 0) << 4);
+        auto it = bucket.find(key);
+        size_t si;
+        if (it == bucket.end()) {
+          GroupStep s;
+          s.type = GroupStep::STATIC;
+          s.f64 = f64s;
+          s.kind = p.kind;
+          s.col = sc.col;
+          s.fwd = fwds;
+          s.L = sc.L;
+          s.tile_start.push_back(0);
+          g->steps.push_back(s);
+          si = g->steps.size() - 1;
+          bucket[key] = si;
+        } else {
+          si = it->second;
+        }
+        GroupStep &s = g->steps[si];
+        const PassArgs pa = pass_args(p, 0, op.in, op.out, op.tw, op.slabs, op.slab);
+        const int tb = static_tile_transforms(h->csize(), sc.L, sc.col);
+        s.sitems.push_back(pa);
+        s.tile_start.push_back(s.tile_start.back() + (pa.total + tb - 1) / tb);
+        s.bytes += pass_bytes(h, p, pa.total);
+        continue;
+      }
       Choice gc;
       B2_TRY(choose_kernel(h->prec, p.kind, p.len, p.batch, p.stride, p.dist, true, &gc));
       GenArgs ga = gc.gen;
@@ -1587,6 +1630,21 @@ int group_build(G *g) {
     return B200FFT_SUCCESS;
   const int sms = sm_count_current();
   for (GroupStep &s : g->steps) {
+    if (s.type != GroupStep::STATIC)
+      continue;
+    cudaError_t e = cudaMalloc(&s.d_sitems, s.sitems.size() * sizeof(PassArgs));
+    if (e == cudaSuccess)
+      e = cudaMalloc(&s.d_tile_start, s.tile_start.size() * sizeof(long long));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(s.d_sitems, s.sitems.data(), s.sitems.size() * sizeof(PassArgs),
+                     cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(s.d_tile_start, s.tile_start.data(),
+                     s.tile_start.size() * sizeof(long long), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "group work list upload");
+  }
+  for (GroupStep &s : g->steps) {
     if (s.type != GroupStep::PASSES)
       continue;
     cudaError_t e = cudaMalloc(&s.d_items, s.items.size() * sizeof(GenArgs));
@@ -1616,7 +1674,7 @@ int group_build(G *g) {
 int group_run(G *g) {
   g->stats.exec_calls++;
   for (GroupStep &s : g->steps) {
-    if (s.type == GroupStep::PASSES) {
+    if (s.type == GroupStep::PASSES || s.type == GroupStep::STATIC) {
       g->stats.kernel_launches++;
       g->stats.bytes_transformed += static_cast<uint64_t>(s.bytes);
     } else {
@@ -1640,6 +1698,20 @@ int group_run(G *g) {
         e = launch_generic_group(s.f64, s.kind, s.col, s.fwd, s.d_items, s.d_tile_start,
                                  static_cast<int>(s.items.size()), g->d_queues + s.queue,
                                  s.smem, s.grid, g->stream);
+    } else if (s.type == GroupStep::STATIC) {
+      what = "grouped specialised pass";
+      const int n = static_cast<int>(s.sitems.size());
+      const long long nt = s.tile_start.back();
+      if (s.kind == KIND_C2C)
+        e = s.f64 ? launch_static_group_c2c_f64(s.L, s.col, s.fwd, s.d_sitems, s.d_tile_start, n,
+                                                nt, g->stream)
+                  : launch_static_group_c2c_f32(s.L, s.col, s.fwd, s.d_sitems, s.d_tile_start, n,
+                                                nt, g->stream);
+      else
+        e = s.f64 ? launch_static_group_real_f64(s.L, s.kind == KIND_R2C, s.d_sitems,
+                                                 s.d_tile_start, n, nt, g->stream)
+                  : launch_static_group_real_f32(s.L, s.kind == KIND_R2C, s.d_sitems,
+                                                 s.d_tile_start, n, nt, g->stream);
     } else if (s.type == GroupStep::COPY) {
       what = "copy";
       e = cudaMemcpyAsync(s.op.dst, s.op.src, s.op.bytes, cudaMemcpyDefault, g->stream);
@@ -1813,7 +1885,7 @@ int b200fft_group_stats(b200fft_group g, b200fft_stats *out) {
   *out = g->stats;
   size_t passes = 0;
   for (const GroupStep &s : g->steps)
-    passes += s.items.size();
+    passes += s.items.size() + s.sitems.size();
   out->exec_calls = g->stats.exec_calls;
   out->coalesced_calls = passes; // passes in the current schedule
   return B200FFT_SUCCESS;

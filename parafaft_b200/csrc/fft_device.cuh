@@ -452,12 +452,13 @@ struct KS {
     }
   }
 
-  static BF_D void entry(const PassArgs &a, V *sm) {
+  // Tile `tile` (TB transforms) of the pass.
+  static BF_D void entry(const PassArgs &a, V *sm, long long tile) {
     Ctx c;
     const int tid = threadIdx.x;
     c.g = COL ? (tid / TB) : (tid % P);
     c.tb = COL ? (tid % TB) : (tid / P);
-    const long long b = static_cast<long long>(blockIdx.x) * TB + c.tb;
+    const long long b = tile * TB + c.tb;
     c.act = b < a.total;
     long long ioff = 0, ooff = 0;
     if (c.act) {
@@ -693,7 +694,30 @@ __global__ void __launch_bounds__(NT, (static_min_blocks<int(sizeof(T) * 2), NT,
     fft_static_kernel(const PassArgs a) {
   using K = KS<T, L, NT, TB, COL, FWD, KIND>;
   extern __shared__ __align__(16) unsigned char smraw[];
-  K::entry(a, reinterpret_cast<typename K::V *>(smraw));
+  K::entry(a, reinterpret_cast<typename K::V *>(smraw), blockIdx.x);
+}
+
+// Grouped specialised pass: the same length and layout for many independent
+// passes (items, e.g. the same stage of many separate grids), each with its
+// own pointers, batch and strides. CTA blockIdx.x runs global tile
+// blockIdx.x; item i covers tiles [tile_start[i], tile_start[i+1]).
+template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND>
+__global__ void __launch_bounds__(NT, (static_min_blocks<int(sizeof(T) * 2), NT, TB, L, COL>()))
+    fft_static_group_kernel(const PassArgs *__restrict__ items,
+                            const long long *__restrict__ tile_start, int nitems) {
+  using K = KS<T, L, NT, TB, COL, FWD, KIND>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const long long t = blockIdx.x;
+  int lo = 0, hi = nitems - 1;
+  while (lo < hi) { // last item whose first tile is <= t
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_start[mid] <= t)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const PassArgs a = items[lo];
+  K::entry(a, reinterpret_cast<typename K::V *>(smraw), t - tile_start[lo]);
 }
 
 template <typename T, int L, int NT, int TB, bool FWD>

@@ -137,6 +137,57 @@ cudaError_t launch_static_var(int var, const PassArgs &a, cudaStream_t st) {
   }
 }
 
+// Grouped specialised pass (full tile): one CTA per tile of every item.
+template <typename T, int L, bool COL, bool FWD, int KIND>
+cudaError_t launch_static_group_one(const PassArgs *items, const long long *tile_start, int nitems,
+                                    long long ntiles, cudaStream_t st) {
+  constexpr CfgS cf = cfg_static(static_cast<int>(sizeof(cvec<T>)), L, COL, 0);
+  using K = KS<T, L, cf.NT, cf.TB, COL, FWD, KIND>;
+  auto kern = fft_static_group_kernel<T, L, cf.NT, cf.TB, COL, FWD, KIND>;
+  constexpr size_t smem = K::smem_bytes();
+  if constexpr (smem > 48 * 1024) {
+    static int configured_mask = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 31 && !(configured_mask & (1 << dev))) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(smem));
+      if (e != cudaSuccess)
+        return e;
+      configured_mask |= (1 << dev);
+    }
+  }
+  if (ntiles <= 0)
+    return cudaSuccess;
+  if (ntiles > INT_MAX)
+    return cudaErrorInvalidConfiguration;
+  kern<<<static_cast<unsigned>(ntiles), cf.NT, smem, st>>>(items, tile_start, nitems);
+  return cudaGetLastError();
+}
+
+#define B2_FG_CASE(LL)                                                         \
+  case LL: return launch_static_group_one<T, LL, COL, FWD, KIND>(items, ts, n, nt, st);
+
+template <typename T, bool COL, bool FWD, int KIND>
+cudaError_t launch_static_group_switch(int L, const PassArgs *items, const long long *ts, int n,
+                                       long long nt, cudaStream_t st) {
+  switch (L) {
+    B2_FG_CASE(2) B2_FG_CASE(4) B2_FG_CASE(8) B2_FG_CASE(16) B2_FG_CASE(32)
+    B2_FG_CASE(64) B2_FG_CASE(128) B2_FG_CASE(256) B2_FG_CASE(512)
+    B2_FG_CASE(1024) B2_FG_CASE(2048)
+    B2_FG_CASE(24) B2_FG_CASE(30) B2_FG_CASE(40) B2_FG_CASE(48) B2_FG_CASE(60)
+    B2_FG_CASE(80) B2_FG_CASE(96) B2_FG_CASE(120) B2_FG_CASE(160) B2_FG_CASE(192)
+    B2_FG_CASE(384) B2_FG_CASE(768)
+  case 4096:
+    if constexpr (KIND == KIND_C2C)
+      return launch_static_group_one<T, 4096, COL, FWD, KIND>(items, ts, n, nt, st);
+    else
+      return cudaErrorInvalidValue;
+  default:
+    return cudaErrorInvalidValue;
+  }
+}
+
 #define B2_FS_CASE(LL)                                                         \
   case LL: return launch_static_var<T, LL, COL, FWD, KIND>(var, a, st);
 

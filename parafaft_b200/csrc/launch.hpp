@@ -20,6 +20,25 @@ cudaError_t launch_static_c2r_f32(int L, int var, const PassArgs &a, cudaStream_
 cudaError_t launch_static_r2c_f64(int L, int var, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_static_c2r_f64(int L, int var, const PassArgs &a, cudaStream_t st);
 
+// Grouped Family S passes (full tile): items are the passes' kernel arguments
+// (device array); item i covers tiles [tile_start[i], tile_start[i+1]) of
+// static_tile_transforms(...) transforms each.
+cudaError_t launch_static_group_c2c_f32(int L, bool col, bool fwd, const PassArgs *items,
+                                        const long long *tile_start, int nitems, long long ntiles,
+                                        cudaStream_t st);
+cudaError_t launch_static_group_c2c_f64(int L, bool col, bool fwd, const PassArgs *items,
+                                        const long long *tile_start, int nitems, long long ntiles,
+                                        cudaStream_t st);
+cudaError_t launch_static_group_real_f32(int L, bool r2c, const PassArgs *items,
+                                         const long long *tile_start, int nitems, long long ntiles,
+                                         cudaStream_t st);
+cudaError_t launch_static_group_real_f64(int L, bool r2c, const PassArgs *items,
+                                         const long long *tile_start, int nitems, long long ntiles,
+                                         cudaStream_t st);
+inline int static_tile_transforms(int esize_complex, int L, bool col) {
+  return cfg_static(esize_complex, L, col, 0).TB;
+}
+
 // Shared-memory bytes of a Family S launch (0 when no kernel exists).
 size_t static_smem_bytes(int esize_complex, int L, bool col, int var);
 

@@ -207,9 +207,11 @@ print(st["kernel_launches"], st["copies_issued"])
 
 
 @pytest.mark.skipif(not _drivers_built(), reason="ParaFaFT drivers not built")
-def test_group_schedules_many_grids_in_six_launches():
+def test_group_schedules_many_grids_per_depth_and_length():
     """256 ParaFaFT_R2C<3> objects of uneven sizes, forward+backward recorded in
-    one group: 6 grouped launches (one per pass depth), 256*6 passes, no copies."""
+    one group: at each of the 6 pass depths one grouped launch per distinct
+    kernel length (every side here has a specialised kernel), 256*6 passes,
+    no copies."""
     out = _run_record(r'''
 import ctypes as C, numpy as np
 from parafaft_b200 import native as nv
@@ -228,9 +230,13 @@ for f, b in zip(objs, bufs):
     f.backward(b.value)
 g.end()
 st = g.stats()
-print(st["kernel_launches"], st["passes_per_run"], st["copies_issued"])
+shapes = [f.shapes()["in_shape"] for f in objs]
+expect = 2 * (len({s[2] for s in shapes}) + len({s[1] for s in shapes}) + len({s[0] for s in shapes}))
+print(st["kernel_launches"], st["passes_per_run"], st["copies_issued"], expect)
 ''')
-    assert out.split() == ["6", str(256 * 6), "0"]
+    launches, passes, copies, expect = out.split()
+    assert launches == expect and passes == str(256 * 6) and copies == "0"
+    assert int(launches) <= 6 * 9
 
 
 def test_wisdom_roundtrip_and_plan_choice(tmp_path):
