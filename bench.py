@@ -44,9 +44,9 @@ ALG_BYTES = 6463422464  # one read + one write per fused pass, fwd+bwd
 
 # DRAM bytes (read + write) per launch from the last `ncu --set full` capture
 # of the same kernels (profiles/r2c512_kernels_ncu_full.md).
-NCU_TRAFFIC = {"r2c_fwd": 1020480000, "c2c_stage1_fwd": 1030265344,
-               "c2c_stage2_fwd": 1029780480, "c2c_stage2_bwd": 1018808576,
-               "c2c_stage1_bwd": 1031222528, "c2r_bwd": 1041284864}
+NCU_TRAFFIC = {"r2c_fwd": 1019973632, "c2c_stage1_fwd": 1030693120,
+               "c2c_stage2_fwd": 1030242048, "c2c_stage2_bwd": 1018437632,
+               "c2c_stage1_bwd": 1030651904, "c2r_bwd": 1040260864}
 
 
 def _peaks():
@@ -584,28 +584,53 @@ def run_b200(args):
     for k in kernels:
         kernels[k]["GBps"] = round(kernels[k]["bytes"] / (kernels[k]["ms"] * 1e-3) / 1e9, 1)
 
-    # ---- end to end through the same API with host buffers
-    for _ in range(max(1, args.warmup // 2)):
-        with torch.cuda.stream(stream):
-            dev.copy_(pinned, non_blocking=True)
-        step()
-        with torch.cuda.stream(stream):
-            result_host.copy_(dev, non_blocking=True)
+    # ---- end to end through the same API with host buffers: every step copies
+    #      its input from pinned host memory, transforms it and reads its result
+    #      back; two device buffers and copy streams let step i's upload overlap
+    #      step i-1's download (PCIe is full duplex), as a user streaming many
+    #      fields would run it
+    dev2 = torch.empty_like(dev)
+    bufs = (dev, dev2)
+    host_in = (pinned, torch.empty_like(pinned).pin_memory())
+    host_in[1].copy_(pinned)
+    host_out = (result_host, torch.empty_like(result_host).pin_memory())
+    s_up, s_down = torch.cuda.Stream(), torch.cuda.Stream()
+    done_down = [torch.cuda.Event(), torch.cuda.Event()]
+
+    def e2e_step(i):
+        k = i & 1
+        d = bufs[k]
+        s_up.wait_event(done_down[k])          # the buffer's previous result is out
+        with torch.cuda.stream(s_up):
+            d.copy_(host_in[k], non_blocking=True)
+        up = torch.cuda.Event()
+        up.record(s_up)
+        stream.wait_event(up)
+        fft.forward(d)
+        fft.backward(d)
+        comp = torch.cuda.Event()
+        comp.record(stream)
+        s_down.wait_event(comp)
+        with torch.cuda.stream(s_down):
+            host_out[k].copy_(d, non_blocking=True)
+        done_down[k].record(s_down)
+
+    for k in range(2):
+        done_down[k].record(s_down)
+    for i in range(max(2, args.warmup // 2)):
+        e2e_step(i)
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            dev.copy_(pinned, non_blocking=True)
-        step()
-        with torch.cuda.stream(stream):
-            result_host.copy_(dev, non_blocking=True)
-    e3.record(stream)
+    e2.record(s_up)
+    for i in range(args.steps):
+        e2e_step(i)
+    e3.record(s_down)
     torch.cuda.synchronize()
     e2e_ms = e2.elapsed_time(e3) / args.steps
+    del dev2
 
     # ---- the split-precision tensor-core form of the same workload: the
     #      column passes (512-point C2C) on the tensor cores, FP16 hi+lo
@@ -659,7 +684,8 @@ def run_b200(args):
                          "peak_source": peak_kind},
             "kernels": kernels,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": nbytes,
-                    "d2h_bytes_per_step": nbytes},
+                    "d2h_bytes_per_step": nbytes,
+                    "pipeline": "two device buffers; step i's upload overlaps step i-1's download"},
             "cufft_backend_ms": cufft_ms if isinstance(cufft_ms, str) else round(cufft_ms, 4),
             "split_tc": split,
             "gpu_launches": int(launches),
