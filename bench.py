@@ -225,6 +225,46 @@ def run_kernels_only(args):
     return 0
 
 
+def run_single_pass(args):
+    """One batched 1D pass of the engine (the command profiled under ncu for a
+    single kernel): FP32 C2C rows / columns or R2C rows of the given length and
+    batch, forward, repeated; prints the plan and the CUDA-event time."""
+    import torch
+    from parafaft_b200 import native as nv
+    kind, length, layout, batch = args.single_pass.split(",")
+    length, batch, col = int(length), int(batch), layout == "col"
+    torch.cuda.set_device(0)
+    h = nv.Handle(nv.F32, 1, flags=nv.FLAG_SPLIT_TC if args.form == "split-tc" else 0)
+    h.set_stream(torch.cuda.current_stream().cuda_stream)  # the events' stream
+    if kind == "c2c":
+        h.plan_c2c(0, length, batch, batch if col else 1, 1 if col else length)
+        d = torch.randn(2 * length * batch, device="cuda")
+        run = lambda: h.exec_c2c(0, nv.FORWARD, d)
+        desc = h.plan_describe(nv.KIND_C2C, 0)
+    else:
+        dist = 2 * (length // 2 + 1)
+        h.plan_r2c(length, batch, 1, dist)
+        d = torch.randn(dist * batch, device="cuda")
+        run = lambda: h.exec_r2c(d)
+        desc = h.plan_describe(nv.KIND_R2C, 0)
+    for _ in range(args.warmup):
+        run()
+    h.sync()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        run()
+    h.flush()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"single_pass": args.single_pass, "form": args.form, "plan": desc,
+                      "ms": round(ms, 4), "GBps": round(2 * d.numel() * 4 / ms / 1e6, 1)}))
+    h.close()
+    return 0
+
+
 C2C_CONFIGS = {
     # name: (shape, precision, orchestrator, input distribution, seed)
     "c2c64": ((64, 64, 64), "f64", "c2c", "uniform", 11),
@@ -718,6 +758,10 @@ def main():
                          "uneven grids; c2c64 / c2c1024 / c2c4d: the C2C configurations")
     ap.add_argument("--grids", type=int, default=256)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--single-pass", default=None, metavar="KIND,LENGTH,LAYOUT,BATCH",
+                    help="profile one engine pass: e.g. c2c,256,row,262144 or r2c,512,row,262144 "
+                         "(layout row = contiguous points, col = neighbouring transforms "
+                         "adjacent); runs --warmup + --steps launches and prints the time")
     ap.add_argument("--form", default="plain", choices=["plain", "split-tc"],
                     help="split-tc: FP32 C2C passes of length 256/512/1024 use the "
                          "split-precision tensor-core kernels (FP16 hi+lo, FP32 accumulate)")
@@ -730,6 +774,8 @@ def main():
         return run_reference(args)
     if args.kernels_only:
         return run_kernels_only(args)
+    if args.single_pass:
+        return run_single_pass(args)
     if args.config == "uneven256":
         return run_uneven(args)
     if args.config in C2C_CONFIGS:
