@@ -582,8 +582,4 @@ cudaError_t launch_tc_c2c_f32(int L, bool col, bool fwd, const PassArgs &a, cuda
   }
 }
 
-size_t tc_smem_bytes(int L, bool col) {
-  return col ? static_cast<size_t>(L) * 16 * 8 : 0;
-}
-
 } // namespace b200fft

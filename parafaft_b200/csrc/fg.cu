@@ -60,12 +60,6 @@ __global__ void twiddle_table_kernel(double2 *t64, float2 *t32, int M, int entri
 
 namespace {
 
-template <typename T> constexpr size_t smem_s(int L, bool col, int var) {
-  const CfgS c = cfg_static(static_cast<int>(sizeof(cvec<T>)), L, col, var);
-  const int LP = col ? L : (L + (L >> (sizeof(cvec<T>) == 8 ? 4 : 3)));
-  return static_cast<size_t>(c.TB) * LP * sizeof(cvec<T>);
-}
-
 template <typename T, bool COL, int KIND, bool FWD>
 cudaError_t launch_g(const GenArgs &g, cudaStream_t st) {
   auto kern = fft_generic_kernel<T, COL, KIND, FWD>;
@@ -162,12 +156,6 @@ cudaError_t launch_generic(bool f64, int kind, bool col, bool fwd,
 
 size_t generic_smem_bytes(bool f64, int TB, int L) {
   return 2ull * TB * L * (f64 ? sizeof(double2) : sizeof(float2));
-}
-
-size_t static_smem_bytes(int esize_complex, int L, bool col, int var) {
-  if (!static_length_ok(L))
-    return 0;
-  return esize_complex == 16 ? smem_s<double>(L, col, var) : smem_s<float>(L, col, var);
 }
 
 int twiddle_table_entries(int n) { return is_pow2(n) ? 2 * n - 1 : n; }

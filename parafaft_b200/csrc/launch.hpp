@@ -39,13 +39,9 @@ inline int static_tile_transforms(int esize_complex, int L, bool col) {
   return cfg_static(esize_complex, L, col, 0).TB;
 }
 
-// Shared-memory bytes of a Family S launch (0 when no kernel exists).
-size_t static_smem_bytes(int esize_complex, int L, bool col, int var);
-
 // Family T: split-precision tensor-core C2C (FP32 data; lengths 256, 512,
 // 1024; row or column tiles).
 cudaError_t launch_tc_c2c_f32(int L, bool col, bool fwd, const PassArgs &a, cudaStream_t st);
-size_t tc_smem_bytes(int L, bool col);
 constexpr bool tc_length_ok(int L) { return L == 256 || L == 512 || L == 1024; }
 // The same on the fifth-generation tensor cores (tcgen05, TMEM accumulators):
 // FP32 C2C rows of length 256.
