@@ -717,14 +717,52 @@ int launch_pass(H *h, const Plan &p, int dir, const void *in, void *out,
 }
 
 // The kernel launch of one pass (no bookkeeping).
+int device_sms(int dev) {
+  static int n[32] = {0};
+  if (dev < 0 || dev >= 32)
+    return 148;
+  if (n[dev] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+      cudaGetLastError();
+      v = 148;
+    }
+    n[dev] = v;
+  }
+  return n[dev];
+}
+
+// Tile of a specialised column pass at launch: a pass too small to give every
+// SM two full tiles (e.g. a 64^3 grid) takes the half or quarter tile, so more
+// CTAs share its latency. Only the Estimate default is adjusted; measured
+// plans keep their choice.
+int column_tile_for(const H *h, const Plan &p, long long total) {
+  int var = p.ch.variant;
+  if (h->plan_flag != B200FFT_PLAN_ESTIMATE || !p.ch.col || !is_pow2(p.ch.L) ||
+      (var != 0 && var != 5))
+    return var;
+  const long long want = 2ll * device_sms(h->device);
+  const int csz = h->csize();
+  if ((total + cfg_static(csz, p.ch.L, true, var).TB - 1) / cfg_static(csz, p.ch.L, true, var).TB >=
+      want)
+    return var;
+  for (int v = 1; v <= 2; ++v)
+    if ((total + cfg_static(csz, p.ch.L, true, v).TB - 1) / cfg_static(csz, p.ch.L, true, v).TB >=
+        want)
+      return v;
+  return 2;
+}
+
 cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
   const bool f64 = h->prec == B200FFT_F64;
   const bool fwd = dir == B200FFT_FORWARD;
   cudaError_t e;
   if (p.ch.family == 0) {
-    if (p.kind == KIND_C2C)
-      e = f64 ? launch_static_c2c_f64(p.ch.L, p.ch.col, fwd, p.ch.variant, a, h->stream)
-              : launch_static_c2c_f32(p.ch.L, p.ch.col, fwd, p.ch.variant, a, h->stream);
+    if (p.kind == KIND_C2C) {
+      const int var = column_tile_for(h, p, a.total);
+      e = f64 ? launch_static_c2c_f64(p.ch.L, p.ch.col, fwd, var, a, h->stream)
+              : launch_static_c2c_f32(p.ch.L, p.ch.col, fwd, var, a, h->stream);
+    }
     else if (p.kind == KIND_R2C)
       e = f64 ? launch_static_r2c_f64(p.ch.L, p.ch.variant, a, h->stream)
               : launch_static_r2c_f32(p.ch.L, p.ch.variant, a, h->stream);
