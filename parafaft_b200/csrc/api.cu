@@ -69,6 +69,7 @@ struct Choice {
   int L = 0;      // complex points of the stage loop
   int tlen = 0;   // twiddle table length
   int TB = 0, NT = 0;
+  int esize = 8;   // bytes per complex element
   int variant = 0; // tile-shape candidate of a specialised kernel
   GenArgs gen{};
 };
@@ -180,6 +181,7 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
                   bool split_tc = false) {
   const int csize = prec == B200FFT_F64 ? 16 : 8;
   Choice ch;
+  ch.esize = csize;
   int L = len;
   bool odd = false;
   if (kind == KIND_C2C) {
@@ -280,14 +282,9 @@ std::string describe_choice(const Choice &ch, int kind) {
   if (ch.family >= 2) {
     rad = (ch.L > 256 ? std::to_string(ch.L / 256) + "x" : std::string()) + "16x16";
   } else if (ch.family == 0) {
-    int m = ch.L;
-    std::vector<int> r;
-    while (m % 8 == 0 && m > 1) { r.push_back(8); m /= 8; }
-    if (m % 4 == 0) { r.push_back(4); m /= 4; }
-    if (m % 2 == 0) { r.push_back(2); m /= 2; }
-    while (m % 5 == 0) { r.push_back(5); m /= 5; }
-    while (m % 3 == 0) { r.push_back(3); m /= 3; }
-    for (size_t i = 0; i < r.size(); ++i)
+    int r[24] = {}, rest = 1;
+    const int n = static_schedule(ch.L, radix_cap(ch.esize, ch.L, ch.TB, ch.NT), r, rest);
+    for (int i = 0; i < n; ++i)
       rad += (i ? "x" : "") + std::to_string(r[i]);
   } else {
     for (int s = 0; s < ch.gen.nst; ++s)

@@ -83,42 +83,75 @@ struct GenArgs {
 };
 
 // ---- compile-time radix schedule for the specialised kernels ------------
-// Radix order: 8s, then one 4 or 2, then 5s, then 3s. Stockham stage s with
-// radix R reads points j + r*L/R and writes (j/Ns)*Ns*R + j%Ns + r*Ns,
-// Ns = product of the radices before s, so the last stage writes natural
-// order directly.
-template <int L> struct SchedS {
+// Stockham stage s with radix R reads points j + r*L/R and writes
+// (j/Ns)*Ns*R + j%Ns + r*Ns, Ns = product of the radices before s, so the last
+// stage writes natural order directly.
+// Powers of two whose threads hold at least 16 points (rmax = 16 or 32) take
+// the fewest stages of radices up to rmax, as even as possible, larger first
+// (1024 = 32x32 or 16x8x8, 512 = 32x16, 256 = 16x16): every stage saved is a
+// shared-memory exchange saved. Otherwise the radix order is 8s, then one 4
+// or 2, then 5s, then 3s. Returns the stage count; `rest` is what no radix
+// divides (1 for a supported length).
+constexpr int static_schedule(int L, int rmax, int (&rad)[24], int &rest) {
+  int k = 0;
+  if (rmax > 8 && L >= 16 && (L & (L - 1)) == 0) {
+    int lg = 0, q = 0;
+    while ((1 << lg) < L)
+      ++lg;
+    while ((1 << q) < rmax)
+      ++q;
+    const int n = (lg + q - 1) / q;
+    for (int i = 0; i < n; ++i)
+      rad[k++] = 1 << (lg / n + (i < lg % n ? 1 : 0));
+    rest = 1;
+    return k;
+  }
+  int m = L;
+  while (m % 8 == 0 && m > 1) {
+    rad[k++] = 8;
+    m /= 8;
+  }
+  if (m % 4 == 0) {
+    rad[k++] = 4;
+    m /= 4;
+  }
+  if (m % 2 == 0) {
+    rad[k++] = 2;
+    m /= 2;
+  }
+  while (m % 5 == 0) {
+    rad[k++] = 5;
+    m /= 5;
+  }
+  while (m % 3 == 0) {
+    rad[k++] = 3;
+    m /= 3;
+  }
+  rest = m;
+  return k;
+}
+
+// Largest radix of a specialised kernel whose threads hold E = L*TB/NT points:
+// the largest power of two <= E between 8 and 32 (16 for 16-byte elements,
+// whose 32-point butterfly would not fit the registers).
+constexpr int radix_cap(int esize, int L, int TB, int NT) {
+  const int e = (L * TB) / NT;
+  const int cap = esize == 8 ? 32 : 16;
+  int r = 8;
+  while (2 * r <= e && 2 * r <= cap)
+    r *= 2;
+  return r;
+}
+
+template <int L, int RMAX = 8> struct SchedS {
   int nst = 0;
   int rad[24] = {};
   int ns[24] = {};
   int rest = 1;
   constexpr SchedS() {
-    int m = L;
-    int k = 0;
-    while (m % 8 == 0 && m > 1) {
-      rad[k++] = 8;
-      m /= 8;
-    }
-    if (m % 4 == 0) {
-      rad[k++] = 4;
-      m /= 4;
-    }
-    if (m % 2 == 0) {
-      rad[k++] = 2;
-      m /= 2;
-    }
-    while (m % 5 == 0) {
-      rad[k++] = 5;
-      m /= 5;
-    }
-    while (m % 3 == 0) {
-      rad[k++] = 3;
-      m /= 3;
-    }
-    rest = m;
-    nst = k;
+    nst = static_schedule(L, RMAX, rad, rest);
     int p = 1;
-    for (int i = 0; i < k; ++i) {
+    for (int i = 0; i < nst; ++i) {
       ns[i] = p;
       p *= rad[i];
     }

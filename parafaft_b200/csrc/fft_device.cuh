@@ -122,6 +122,114 @@ template <bool FWD, typename V> BF_D void dft8(V *v) {
   v[7] = csub(e3, o3);
 }
 
+// ---- 16- and 32-point butterflies from 4- and 8-point ones ---------------
+// cos and sin of 2*pi*m/n at compile time: the angle is folded by symmetry
+// into [0, pi/4] with exact integer arithmetic (in units of 1/(8n) turn), then
+// summed from the Taylor series (16 terms: far below double rounding there).
+struct CosSin {
+  double c, s;
+};
+constexpr CosSin ce_cossin(long long m, long long n) {
+  m %= n;
+  if (m < 0)
+    m += n;
+  long long a = 8 * m, d = 8 * n; // angle = 2*pi*a/d
+  bool neg_s = false, neg_c = false, swap = false;
+  if (2 * a > d) { // 2*pi - x
+    a = d - a;
+    neg_s = true;
+  }
+  if (4 * a > d) { // pi - x
+    a = d / 2 - a;
+    neg_c = true;
+  }
+  if (8 * a > d) { // pi/2 - x
+    a = d / 4 - a;
+    swap = true;
+  }
+  const double x = 2.0 * 3.14159265358979323846264338327950288 * static_cast<double>(a) /
+                   static_cast<double>(d);
+  double ts = x, ss = x, tc = 1.0, sc = 1.0;
+  for (int k = 1; k < 16; ++k) {
+    ts *= -x * x / static_cast<double>((2 * k) * (2 * k + 1));
+    tc *= -x * x / static_cast<double>((2 * k - 1) * (2 * k));
+    ss += ts;
+    sc += tc;
+  }
+  double c = swap ? ss : sc, sn = swap ? sc : ss;
+  return CosSin{neg_c ? -c : c, neg_s ? -sn : sn};
+}
+template <int M, int N> struct TwC {
+  static constexpr double c = ce_cossin(M, N).c;
+  static constexpr double s = ce_cossin(M, N).s;
+};
+
+// a * exp(-+2*pi*i*M/N) for compile-time M, N (forward: minus). Multiples of
+// an eighth of a turn cost at most two multiplications.
+template <int M, int N, bool FWD, typename V> BF_D V twk(V a) {
+  using T = decltype(a.x);
+  constexpr int m = ((M % N) + N) % N;
+  constexpr T h = T(0.70710678118654752440084436210485);
+  if constexpr (m == 0) {
+    return a;
+  } else if constexpr (4 * m == N) {
+    return rot<FWD>(a);
+  } else if constexpr (2 * m == N) {
+    return cmake(-a.x, -a.y);
+  } else if constexpr (4 * m == 3 * N) {
+    return rot<!FWD>(a);
+  } else if constexpr (8 * m == N || 8 * m == 5 * N) {
+    const V b = FWD ? cmake(h * (a.x + a.y), h * (a.y - a.x))
+                    : cmake(h * (a.x - a.y), h * (a.x + a.y));
+    return 8 * m == N ? b : cmake(-b.x, -b.y);
+  } else if constexpr (8 * m == 3 * N || 8 * m == 7 * N) {
+    const V b = FWD ? cmake(h * (a.y - a.x), -h * (a.x + a.y))
+                    : cmake(-h * (a.x + a.y), h * (a.x - a.y));
+    return 8 * m == 3 * N ? b : cmake(-b.x, -b.y);
+  } else {
+    constexpr T c = T(TwC<m, N>::c), sn = T(TwC<m, N>::s);
+    return FWD ? cmake(a.x * c + a.y * sn, a.y * c - a.x * sn)
+               : cmake(a.x * c - a.y * sn, a.y * c + a.x * sn);
+  }
+}
+
+template <int R, bool FWD, typename V> BF_D void dft(V *v);
+
+// N = N1*N2 points in natural order: n = N2*n1 + n2, k = k1 + N1*k2;
+// N2 DFTs of N1 points over n1, the twiddles w_N^(n2*k1), then N1 DFTs of
+// N2 points over n2.
+template <int N1, int N2, bool FWD, typename V> struct CompositeDft {
+  static constexpr int N = N1 * N2;
+  template <int n2, int k1> static BF_D void twiddle_into(const V *u, V *t) {
+    if constexpr (k1 < N1) {
+      t[k1 * N2 + n2] = twk<n2 * k1, N, FWD>(u[k1]);
+      twiddle_into<n2, k1 + 1>(u, t);
+    }
+  }
+  template <int n2> static BF_D void inner(const V *v, V *t) {
+    if constexpr (n2 < N2) {
+      V u[N1];
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1)
+        u[n1] = v[N2 * n1 + n2];
+      dft<N1, FWD>(u);
+      twiddle_into<n2, 0>(u, t);
+      inner<n2 + 1>(v, t);
+    }
+  }
+  static BF_D void run(V *v) {
+    V t[N];
+    inner<0>(v, t);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+      dft<N2, FWD>(&t[k1 * N2]);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2)
+        v[k1 + N1 * k2] = t[k1 * N2 + k2];
+    }
+  }
+};
+
 template <int R, bool FWD, typename V> BF_D void dft(V *v) {
   if constexpr (R == 1) {
   } else if constexpr (R == 2) {
@@ -134,6 +242,10 @@ template <int R, bool FWD, typename V> BF_D void dft(V *v) {
     dft5<FWD>(v);
   } else if constexpr (R == 8) {
     dft8<FWD>(v);
+  } else if constexpr (R == 16) {
+    CompositeDft<4, 4, FWD, V>::run(v);
+  } else if constexpr (R == 32) {
+    CompositeDft<4, 8, FWD, V>::run(v);
   } else {
     static_assert(R == 0, "unsupported radix");
   }
@@ -209,6 +321,31 @@ BF_D void apply_twiddles_pyr(V *v, const V *tn, int n, int k) {
     v[5] = cmulw<CONJ>(v[5], cmulw<false>(w4, w1));
     v[6] = cmulw<CONJ>(v[6], cmulw<false>(w4, w2));
     v[7] = cmulw<CONJ>(v[7], cmulw<false>(w4, w3));
+  } else if constexpr (R == 16 || R == 32) {
+    // w^(2^b) from the levels n/2^b, the other powers as products of those
+    // (at most four factors for R = 32)
+    V w[R];
+    w[1] = ldtw(tn, k);
+    w[2] = ldtw(tn, n + k);
+    w[4] = ldtw(tn, n + n / 2 + k);
+    w[8] = ldtw(tn, n + n / 2 + n / 4 + k);
+    if constexpr (R == 32)
+      w[16] = ldtw(tn, n + n / 2 + n / 4 + n / 8 + k);
+    w[3] = cmulw<false>(w[1], w[2]);
+#pragma unroll
+    for (int r = 5; r < 8; ++r)
+      w[r] = cmulw<false>(w[4], w[r - 4]);
+#pragma unroll
+    for (int r = 9; r < 16; ++r)
+      w[r] = cmulw<false>(w[8], w[r - 8]);
+    if constexpr (R == 32) {
+#pragma unroll
+      for (int r = 17; r < 32; ++r)
+        w[r] = cmulw<false>(w[16], w[r - 16]);
+    }
+#pragma unroll
+    for (int r = 1; r < R; ++r)
+      v[r] = cmulw<CONJ>(v[r], w[r]);
   } else {
 #pragma unroll
     for (int r = 1; r < R; ++r)
@@ -230,7 +367,8 @@ template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND,
           bool STAGED = false>
 struct KS {
   using V = cvec<T>;
-  static constexpr SchedS<L> S{};
+  // radices up to the points a thread holds (32 / 16 at most)
+  static constexpr SchedS<L, radix_cap(int(sizeof(V)), L, TB, NT)> S{};
   static constexpr int NST = S.nst;
   static constexpr int P = NT / TB; // threads per transform
   // Row layouts pad one element every 16 (8-byte elements) or 8 (16-byte
