@@ -166,9 +166,17 @@ int ilog2(int x) {
 int default_variant(int csize, int L, bool col, long long stride) {
   if (col && stride * csize >= (4ll << 20))
     return 3;
-  // FP32 columns of 512+ points: 512-thread full tiles, two CTAs per SM
+  // FP32 columns of 1024 points: the full tile, 32 points per thread, two
+  // 32-point stages
+  if (col && csize == 8 && L == 1024)
+    return 0;
+  // other FP32 columns of 512+ points: 512-thread full tiles, two CTAs per SM
   if (col && csize == 8 && L >= 512)
     return 5;
+  // FP32 rows of 256 and 512 points: twice the points per thread (16 and 32),
+  // so the radix-16/32 schedule needs two stages instead of three
+  if (!col && csize == 8 && (L == 256 || L == 512))
+    return 1;
   return 0;
 }
 
