@@ -44,9 +44,9 @@ ALG_BYTES = 6463422464  # one read + one write per fused pass, fwd+bwd
 
 # DRAM bytes (read + write) per launch from the last `ncu --set full` capture
 # of the same kernels (profiles/r2c512_kernels_ncu_full.md).
-NCU_TRAFFIC = {"r2c_fwd": 1019973632, "c2c_stage1_fwd": 1030693120,
-               "c2c_stage2_fwd": 1030242048, "c2c_stage2_bwd": 1018437632,
-               "c2c_stage1_bwd": 1030651904, "c2r_bwd": 1040260864}
+NCU_TRAFFIC = {"r2c_fwd": 1021177600, "c2c_stage1_fwd": 1030037504,
+               "c2c_stage2_fwd": 1029770496, "c2c_stage2_bwd": 1018680320,
+               "c2c_stage1_bwd": 1030023168, "c2r_bwd": 1039329024}
 
 
 def _peaks():
@@ -209,10 +209,45 @@ def run_reference(args):
 
 def run_kernels_only(args):
     """The timed loop alone (no checks, no comparators): the command profiled
-    under ncu."""
+    under ncu. --config picks the workload: r2c512 (default), c2c64 / c2c1024 /
+    c2c4d (forward+backward of that grid), uneven256 (the grouped schedule of
+    the uneven grids captured in a CUDA graph and replayed)."""
     import torch
     from parafaft_b200 import native as nv
     torch.cuda.set_device(0)
+    if args.config in C2C_CONFIGS:
+        shape, prec_s, kind, _, seed = C2C_CONFIGS[args.config]
+        prec = nv.F64 if prec_s == "f64" else nv.F32
+        f = nv.ParaFaFT(kind, shape, prec)
+        gen = torch.Generator(device="cuda").manual_seed(seed)
+        data = torch.randn(f.required_size, generator=gen, device="cuda",
+                           dtype=torch.complex128 if prec == nv.F64 else torch.complex64)
+        for _ in range(args.warmup + args.steps):
+            f.forward(data)
+            f.backward(data)
+        torch.cuda.synchronize()
+        print("kernels-only done", f.handle().stats()["kernel_launches"])
+        f.close()
+        return 0
+    if args.config == "uneven256":
+        rng = np.random.default_rng(args.seed)
+        shapes = [tuple(int(s) for s in rng.choice(UNEVEN_SIDES, 3)) for _ in range(args.grids)]
+        objs = [nv.ParaFaFT("r2c", shp, nv.F32) for shp in shapes]
+        gen = torch.Generator(device="cuda").manual_seed(args.seed)
+        devs = [torch.randn(f.required_size, generator=gen, device="cuda") for f in objs]
+        g = nv.Group([f.handle() for f in objs])
+        g.begin()
+        for f, d in zip(objs, devs):
+            f.forward(d)
+            f.backward(d)
+        g.end()
+        g.sync()
+        g.capture()
+        for _ in range(args.warmup + args.steps):
+            g.replay()
+        g.sync()
+        print("kernels-only done", g.stats()["kernel_launches"])
+        return 0
     host_buf, _ = make_input()
     fft = nv.ParaFaFT("r2c", SHAPE, nv.F32)
     dev = torch.from_numpy(host_buf).cuda()
