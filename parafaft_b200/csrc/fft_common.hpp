@@ -158,6 +158,112 @@ template <int L, int RMAX = 8> struct SchedS {
   }
 };
 
+constexpr int ce_min(int a, int b) { return a < b ? a : b; }
+constexpr int ce_max(int a, int b) { return a > b ? a : b; }
+
+// ---- shared-memory layout of row tiles -----------------------------------
+// A row tile keeps point n of its transform tb at tb*lp + n + (n >> sh): a pad
+// element every 2^sh points and a row pitch lp. One element in 16 (8-byte) or
+// 8 (16-byte) with lp = L + L/16 suits power-of-two rows; other lengths pick
+// (sh, lp) here by scoring every candidate (sh in {2, 3, 4, 5, none}, lp from
+// the smallest pitch up by 15) on the exchange accesses of warp 0: the
+// Stockham writes and reads between stages and, for R2C rows, the Hermitian
+// pair reads. 8-byte elements fall on 16 bank pairs, 16-byte ones on 8 bank
+// quads; an access costs the largest number of lanes on one of them (the
+// shared-memory wavefronts it takes).
+struct RowPad {
+  int sh, lp;
+};
+
+template <class Sch>
+constexpr long long row_pad_cost(const Sch &S, int L, int P, int esize, bool post, int sh,
+                                 int lp) {
+  const int nb = 128 / esize;
+  long long cost = 0;
+  int cnt[16] = {};
+  for (int s = 0; s < S.nst; ++s) {
+    const int R = S.rad[s], Ns = S.ns[s], B = L / R;
+    const bool last = s == S.nst - 1;
+    for (int phase = 0; phase < 2; ++phase) { // writes of stage s, reads of s+1
+      if ((phase == 0 && last && !post) || (phase == 1 && last))
+        continue;
+      const int Rx = phase == 0 ? R : S.rad[s + 1];
+      const int Bx = L / Rx;
+      const int Kx = (Bx + P - 1) / P;
+      for (int i = 0; i < Kx; ++i)
+        for (int r = 0; r < Rx; ++r) {
+          for (int b = 0; b < nb; ++b)
+            cnt[b] = 0;
+          for (int l = 0; l < 32; ++l) {
+            const int g = P <= 32 ? l % P : l, tb = P <= 32 ? l / P : 0;
+            const int j = g + P * i;
+            if (j >= Bx)
+              continue;
+            const int n = phase == 1 ? j + r * Bx
+                          : last     ? j + r * B
+                                     : (j / Ns) * Ns * R + j % Ns + r * Ns;
+            ++cnt[(tb * lp + n + (n >> sh)) % nb];
+          }
+          int mx = 0;
+          for (int b = 0; b < nb; ++b)
+            mx = cnt[b] > mx ? cnt[b] : mx;
+          cost += mx;
+        }
+    }
+  }
+  if (post) { // R2C: X[k] reads Z[k] and Z[L-k] (k = 0..L, 0 for L)
+    const int KO = (L + 1 + P - 1) / P;
+    for (int i = 0; i < KO; ++i)
+      for (int h = 0; h < 2; ++h) {
+        for (int b = 0; b < nb; ++b)
+          cnt[b] = 0;
+        for (int l = 0; l < 32; ++l) {
+          const int g = P <= 32 ? l % P : l, tb = P <= 32 ? l / P : 0;
+          const int k = g + P * i;
+          if (k > L)
+            continue;
+          const int n = h == 0 ? (k == L ? 0 : k) : (k == 0 ? 0 : L - k);
+          ++cnt[(tb * lp + n + (n >> sh)) % nb];
+        }
+        int mx = 0;
+        for (int b = 0; b < nb; ++b)
+          mx = cnt[b] > mx ? cnt[b] : mx;
+        cost += mx;
+      }
+  }
+  return cost;
+}
+
+// The layout of a row tile of TB transforms (the cheapest candidate whose tile
+// stays within 48 KiB or within the default layout's size; ties keep the
+// default, then the smaller pitch).
+template <class Sch>
+constexpr RowPad choose_row_pad(const Sch &S, int L, int P, int TB, int esize, bool post,
+                                bool search) {
+  const int sh0 = esize == 8 ? 4 : 3;
+  RowPad best{sh0, L + (L >> sh0)};
+  if (!search)
+    return best;
+  const long long budget = ce_max(48 * 1024, TB * best.lp * esize);
+  long long bc = row_pad_cost(S, L, P, esize, post, best.sh, best.lp);
+  const int shs[5] = {2, 3, 4, 5, 30};
+  for (int a = 0; a < 5; ++a) {
+    const int sh = shs[a];
+    const int base = (L - 1) + ((L - 1) >> sh) + 1;
+    for (int q = 0; q < 16; ++q) {
+      const int lp = base + q;
+      if (static_cast<long long>(TB) * lp * esize > budget)
+        break;
+      const long long c = row_pad_cost(S, L, P, esize, post, sh, lp);
+      if (c < bc) {
+        bc = c;
+        best = RowPad{sh, lp};
+      }
+    }
+  }
+  return best;
+}
+
 // Configuration of a specialised kernel: NT threads, TB transforms per CTA,
 // P = NT/TB threads per transform, E points per thread.
 //  * column layout (points strided, neighbouring transforms adjacent in
@@ -170,8 +276,6 @@ struct CfgS {
   int NT, TB, P, E;
 };
 
-constexpr int ce_min(int a, int b) { return a < b ? a : b; }
-constexpr int ce_max(int a, int b) { return a > b ? a : b; }
 
 // `variant` selects the tile shape among the candidates the planner (and its
 // autotuner) choose from:

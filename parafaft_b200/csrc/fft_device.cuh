@@ -371,11 +371,6 @@ struct KS {
   static constexpr SchedS<L, radix_cap(int(sizeof(V)), L, TB, NT)> S{};
   static constexpr int NST = S.nst;
   static constexpr int P = NT / TB; // threads per transform
-  // Row layouts pad one element every 16 (8-byte elements) or 8 (16-byte
-  // elements) so that both contiguous reads and the stride-R writes of the
-  // Stockham stages hit every bank equally.
-  static constexpr int PADSH = sizeof(V) == 8 ? 4 : 3;
-  static constexpr int LP = COL ? L : (L + (L >> PADSH));
   static constexpr int TSCALE = (KIND == KIND_C2C) ? 1 : 2;
   static constexpr bool WARP_SYNC = !COL && (P <= 32) && (32 % P == 0);
   static_assert(NT % TB == 0, "TB must divide NT");
@@ -406,6 +401,16 @@ struct KS {
   // point P*(L/P - m)), so R2C/C2R pair points with warp shuffles instead of
   // a pass through shared memory.
   static constexpr bool SHUF = !COL && KIND != KIND_C2C && P <= 32 && all_full();
+  // Row layouts: power-of-two lengths pad one element every 16 (8-byte
+  // elements) or 8 (16-byte elements) so that both contiguous reads and the
+  // stride-R writes of the Stockham stages hit every bank equally; other
+  // lengths take the layout with the fewest shared-memory wavefronts on their
+  // own access pattern (choose_row_pad).
+  static constexpr RowPad RP = choose_row_pad(S, L, P, TB, int(sizeof(V)),
+                                              KIND == KIND_R2C && !SHUF,
+                                              !COL && (L & (L - 1)) != 0);
+  static constexpr int PADSH = RP.sh;
+  static constexpr int LP = COL ? L : RP.lp;
   static constexpr int TM = L * TSCALE; // top length of the twiddle pyramid
 
   static constexpr size_t smem_bytes() {
