@@ -829,7 +829,9 @@ struct KS {
 // C2C of 256 points) fit four CTAs per SM (64 registers).
 template <int ES, int NT, int TB, int L, bool COL> constexpr int static_min_blocks() {
   return NT == 256 ? (COL ? B2_COL_MIN_BLOCKS
-                          : ((TB * L) / NT <= 8 && ES == 8 ? 4 : B2_ROW_MIN_BLOCKS))
+                          : ((TB * L) / NT <= 8 && ES == 8    ? 4
+                             : (TB * L) / NT <= 16 && ES == 8 ? 3
+                                                              : B2_ROW_MIN_BLOCKS))
                    : ((ES == 8 && COL && NT == 512 && (TB * L) / NT <= 16) ? 2 : 1);
 }
 template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND>
