@@ -92,7 +92,9 @@ typedef struct b200fft_launch_record {
   int kind;          /* 0 c2c, 1 r2c, 2 c2r, 3 copy                         */
   int direction;     /* B200FFT_FORWARD / B200FFT_BACKWARD                   */
   int stage;         /* stage index for c2c, -1 otherwise                    */
-  int family;        /* 0 static specialised kernel, 1 runtime generic, -1 copy */
+  int family;        /* 0 static specialised kernel, 1 runtime generic,
+                        2/3 split-precision tensor core (mma.sync / tcgen05),
+                        4 TMA-fed specialised column kernel, -1 copy */
   int length;        /* transform length (real length for r2c/c2r)          */
   int fused_copy;    /* 1 when the transform read a held-back copy's source */
   long long transforms; /* 1D transforms in the launch (batch x slabs)      */

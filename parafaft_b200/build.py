@@ -34,7 +34,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC"] + ARCH
 
 ENGINE_SOURCES = ["api.cu", "fg.cu", "fs_c2c_f32.cu", "fs_c2c_f64.cu",
-                  "fs_r2c_f32.cu", "fs_r2c_f64.cu", "fft_tc.cu", "fft_tc5.cu", "noalloc.cu"]
+                  "fs_r2c_f32.cu", "fs_r2c_f64.cu", "fft_tc.cu", "fft_tc5.cu", "fft_tma.cu",
+                  "noalloc.cu"]
 
 
 def _nvcc() -> str:

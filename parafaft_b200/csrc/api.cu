@@ -332,6 +332,8 @@ struct b200fft_handle_s {
   bool force_generic = false;
   bool split_tc = false; // split-precision tensor-core kernels where they exist
   bool used_tc5 = false; // launched a tcgen05 kernel (check its fault word at sync)
+  bool used_tma = false; // launched a TMA column kernel (check its fault word at sync)
+  bool last_tma = false; // the last transform launch ran the TMA column kernel
   int device = -1;
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
@@ -713,7 +715,10 @@ int launch_pass(H *h, const Plan &p, int dir, const void *in, void *out,
     return B200FFT_SUCCESS;
   }
   ProfileScope ps(h);
+  h->last_tma = false;
   const cudaError_t e = launch_kernel(h, p, dir, a);
+  if (h->last_tma)
+    r.family = 4;
   push_log(h, r);
   ps.done();
   if (e != cudaSuccess)
@@ -764,7 +769,16 @@ cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
   cudaError_t e;
   if (p.ch.family == 0) {
     if (p.kind == KIND_C2C) {
-      const int var = column_tile_for(h, p, a.total);
+      int var = column_tile_for(h, p, a.total);
+      if (var == kVariantTma || var == kVariantTma + 1) {
+        if (!f64 && p.ch.col && tma_col_ok(p.ch.L, a)) {
+          h->used_tma = true;
+          h->last_tma = true;
+          return launch_tma_col_c2c_f32(p.ch.L, fwd, var == kVariantTma ? 512 : 1024, a,
+                                        h->stream);
+        }
+        var = default_variant(h->csize(), p.ch.L, p.ch.col, p.stride);
+      }
       e = f64 ? launch_static_c2c_f64(p.ch.L, p.ch.col, fwd, var, a, h->stream)
               : launch_static_c2c_f32(p.ch.L, p.ch.col, fwd, var, a, h->stream);
     }
@@ -933,8 +947,8 @@ int autotune(H *h, Plan &p) {
   std::vector<std::pair<int, int>> cands; // (family, variant)
   if (p.ch.family == 0) {
     if (p.ch.col) {
-      const int meas[] = {0, 3, 5};
-      const int pat[] = {0, 1, 2, 3, 4, 5, 6, 7};
+      const int meas[] = {0, 3, 5, 8};
+      const int pat[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9};
       if (rigor >= B200FFT_PLAN_PATIENT)
         for (int v : pat) cands.push_back({0, v});
       else
@@ -1331,6 +1345,16 @@ int b200fft_sync(b200fft_handle h) {
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess)
     return cuda_fail(e, "cudaStreamSynchronize");
+  if (h->used_tma) {
+    unsigned fault = 0;
+    e = tma_take_fault(&fault);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "TMA column kernel fault word");
+    if (fault)
+      return fail(B200FFT_ERR_DEVICE_STATUS,
+                  "b200fft: a TMA column kernel gave up waiting for its tile copies "
+                  "(results of that launch are invalid)");
+  }
   if (h->used_tc5) {
     unsigned fault = 0;
     e = tc5_take_fault(&fault);

@@ -292,7 +292,13 @@ struct CfgS {
 //       current one is transformed (two CTAs per SM).
 //   7 = wide column tile on 1024 threads (twice the full tile, half the
 //       points per thread): wide row segments with 32 warps per SM.
-constexpr int kStaticVariants = 8;
+//   8 = TMA-fed column pass (FP32, 256/512/1024 points, 16-byte aligned
+//       rows): persistent CTAs of 512 threads stream 64 KiB tiles through a
+//       ring of three shared-memory buffers filled by bulk tensor copies;
+//   9 = the same on 1024 threads per CTA.
+// Where a TMA variant does not apply, the plan's default tile runs instead.
+constexpr int kStaticVariants = 10;
+constexpr int kVariantTma = 8;
 constexpr int kVariantStaged = 4;
 constexpr int kVariantPipelined = 6;
 
@@ -317,11 +323,11 @@ constexpr CfgS cfg_static(int esize, int L, bool col, int variant = 0) {
     const int P = ce_min(NT, floor_pow2(ce_max(1, L / 8)));
     return CfgS{NT, NT / P, P, (L + P - 1) / P};
   }
-  const int NT = (col && variant == 7) ? 1024
-                 : (col && (variant >= 3 && variant <= 5)) ? 512 : 256;
+  const int NT = (col && (variant == 7 || variant == 9)) ? 1024
+                 : (col && ((variant >= 3 && variant <= 5) || variant == 8)) ? 512 : 256;
   const int base = esize == 8 ? 8192 : 4096;
   const int target = col ? ((variant == 3 || variant == 7) ? 2 * base
-                                         : (variant == 4 || variant == 5)
+                                         : (variant == 4 || variant == 5 || variant >= 8)
                                                ? base
                                                : variant == 6 ? base / 2 : (base >> variant))
                          : base;

@@ -1,0 +1,296 @@
+// TMA-fed column passes: FP32 C2C of 256, 512 or 1024 points whose point
+// rows are 16-byte aligned (ParaFaFT's first axis, and middle axes of even
+// width).
+//
+// A persistent CTA per SM walks its tiles (TB adjacent transforms, 64 KiB)
+// through a ring of three shared-memory buffers. Thread 0 fills each buffer
+// with bulk tensor copies (cp.async.bulk.tensor, one per 256 point rows, box
+// {TB columns, rows, 1 slab} of a 3D map {columns, points, slabs}) that
+// complete on the buffer's mbarrier; while the CTA transforms tile t, the
+// copies of tiles t+1 and t+2 are in flight, so the load phase of one tile
+// overlaps the arithmetic of the previous ones inside the SM instead of
+// across co-resident CTAs. The TMA box lands as [point][transform], which is
+// the column layout of the Stockham stages (KS::sidx): stage 0 reads its
+// points from the buffer, the later stages exchange through the same buffer,
+// and the last stage stores to global memory directly.
+//
+// Every wait on a buffer's barrier is bounded by the clock (about a second);
+// past it the CTA sets g_tma_fault, waits (bounded) for the copies it still
+// has in flight and returns, and b200fft_sync reports
+// B200FFT_ERR_DEVICE_STATUS. B200FFT_TMA_STALL_TEST=1 makes every CTA skip the
+// copies of its first tile, so that first wait runs out (the test of this
+// path: nothing faults, the context stays usable).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <cstdlib>
+#include <mutex>
+
+#include "fs_launch.cuh"
+
+namespace b200fft {
+
+__device__ unsigned int g_tma_fault = 0;
+
+namespace {
+
+constexpr int kTmaStages = 3;
+constexpr int kTmaTileBytes = 64 * 1024; // one tile: 8192 complex64
+constexpr int kTmaMaxRows = 256;         // box height limit of a tensor copy
+constexpr int kTmaSmem = kTmaStages * kTmaTileBytes;
+
+BF_D uint32_t su32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Phase `parity` of the barrier, at most about a second of clock.
+BF_D bool tma_wait(uint32_t mbar, uint32_t parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred P1;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+                 "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                 : "=r"(done)
+                 : "r"(mbar), "r"(parity), "r"(1000u)
+                 : "memory");
+    if (done)
+      return true;
+    if (clock64() - t0 > (2ll << 30))
+      return false;
+  }
+}
+
+template <int L, int NT, bool FWD>
+__global__ void __launch_bounds__(NT, 1)
+    fft_tma_col_kernel(const __grid_constant__ CUtensorMap map, const PassArgs a,
+                       long long tiles_per_slab, int stall) {
+  constexpr int TB = kTmaTileBytes / (L * 8);
+  constexpr int ROWS = L < kTmaMaxRows ? L : kTmaMaxRows;
+  using K = KS<float, L, NT, TB, true, FWD, KIND_C2C, true>;
+  using V = typename K::V;
+  static_assert(TB * L * 8 == kTmaTileBytes, "a tile fills one ring buffer");
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  __shared__ __align__(8) unsigned long long full[kTmaStages];
+  __shared__ int abort_flag;
+  V *const ring = reinterpret_cast<V *>(smraw);
+  const long long slabs = a.total / a.batch;
+  const long long ntiles = slabs * tiles_per_slab;
+  const long long G = gridDim.x;
+  const int tid = threadIdx.x;
+  if (static_cast<long long>(blockIdx.x) >= ntiles)
+    return;
+
+  // thread 0: the copies of tile `tile` into buffer s, completing on full[s]
+  auto issue = [&](long long tile, int s) {
+    const long long sl = tile / tiles_per_slab;
+    const int x = static_cast<int>((tile - sl * tiles_per_slab) * TB * 2); // floats
+    const uint32_t mb = su32(&full[s]);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
+                 "r"(kTmaTileBytes)
+                 : "memory");
+#pragma unroll
+    for (int y = 0; y < L; y += ROWS) {
+      const uint32_t dst = su32(ring + static_cast<size_t>(s) * L * TB + y * TB);
+      asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                   " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+                   "l"(reinterpret_cast<uint64_t>(&map)), "r"(x), "r"(y),
+                   "r"(static_cast<int>(sl)), "r"(mb)
+                   : "memory");
+    }
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < kTmaStages; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&full[s])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int s = 0; s < kTmaStages; ++s) {
+      const long long t = blockIdx.x + s * G;
+      if (t < ntiles && !(stall && s == 0))
+        issue(t, s);
+    }
+
+  typename K::Ctx c;
+  c.g = tid / TB;
+  c.tb = tid % TB;
+  c.tw = reinterpret_cast<const V *>(a.tw);
+  c.ist = a.istride;
+  c.ost = a.ostride;
+  c.gin = nullptr;
+  for (long long it = 0;; ++it) {
+    const long long tile = blockIdx.x + it * G;
+    if (tile >= ntiles)
+      break;
+    const int s = static_cast<int>(it % kTmaStages);
+    const uint32_t parity = static_cast<uint32_t>((it / kTmaStages) & 1);
+    if (tid == 0 && !tma_wait(su32(&full[s]), parity)) {
+      abort_flag = 1;
+      atomicOr(&g_tma_fault, 1u);
+    }
+    __syncthreads();
+    if (abort_flag) {
+      // the copies of the later tiles this CTA issued may still be running:
+      // wait for them (bounded) before the CTA's shared memory goes away
+      if (tid == 0)
+        for (int k = 1; k < kTmaStages; ++k) {
+          const long long later = it + k;
+          if (blockIdx.x + later * G < ntiles)
+            tma_wait(su32(&full[later % kTmaStages]),
+                     static_cast<uint32_t>((later / kTmaStages) & 1));
+        }
+      return;
+    }
+    c.sm = ring + static_cast<size_t>(s) * L * TB;
+    const long long sl = tile / tiles_per_slab;
+    const long long w = (tile - sl * tiles_per_slab) * TB + c.tb;
+    c.act = w < a.batch;
+    c.gout = reinterpret_cast<V *>(a.out) + (c.act ? sl * a.oslab + w * a.odist : 0);
+    V v[K::EMAX];
+    constexpr int R = K::S.rad[0];
+    constexpr int B = L / R;
+    constexpr int KB = (B + K::P - 1) / K::P;
+    constexpr bool FULL = (B % K::P) == 0;
+#pragma unroll
+    for (int i = 0; i < KB; ++i) {
+      const int j = c.g + K::P * i;
+      if (FULL || j < B) {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          v[i * R + r] = c.sm[(j + r * B) * TB + c.tb];
+      }
+    }
+    K::template run<0>(c, v);
+    __syncthreads(); // every thread is done with buffer s
+    if (tid == 0) {
+      const long long next = tile + kTmaStages * G;
+      if (next < ntiles) {
+        // the buffer was last written through the generic proxy (the stage
+        // exchanges): order those writes before the async proxy's refill
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(next, s);
+      }
+    }
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+template <int L, int NT, bool FWD>
+cudaError_t launch_tma_t(const PassArgs &a, cudaStream_t st) {
+  constexpr int TB = kTmaTileBytes / (L * 8);
+  constexpr int ROWS = L < kTmaMaxRows ? L : kTmaMaxRows;
+  auto kern = fft_tma_col_kernel<L, NT, FWD>;
+  static int configured_mask = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 31 && !(configured_mask & (1 << dev))) {
+    cudaError_t e =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem);
+    if (e != cudaSuccess)
+      return e;
+    configured_mask |= (1 << dev);
+  }
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (enc == nullptr)
+    return cudaErrorNotSupported;
+  const long long slabs = a.total / a.batch;
+  // {columns (floats), points, slabs}; strides in bytes for dims 1 and 2
+  const cuuint64_t dims[3] = {static_cast<cuuint64_t>(2 * a.batch), static_cast<cuuint64_t>(L),
+                              static_cast<cuuint64_t>(slabs)};
+  const cuuint64_t strides[2] = {static_cast<cuuint64_t>(a.istride) * 8,
+                                 static_cast<cuuint64_t>(slabs > 1 ? a.islab
+                                                                   : a.istride * L) * 8};
+  const cuuint32_t box[3] = {static_cast<cuuint32_t>(2 * TB), static_cast<cuuint32_t>(ROWS), 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUtensorMap map;
+  const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(a.in),
+                         dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  const long long tps = (a.batch + TB - 1) / TB;
+  const long long ntiles = tps * slabs;
+  if (ntiles <= 0)
+    return cudaSuccess;
+  const long long sms = sm_count();
+  const long long grid = ntiles < sms ? ntiles : sms;
+  const char *sv = std::getenv("B200FFT_TMA_STALL_TEST");
+  const int stall = (sv != nullptr && sv[0] == '1') ? 1 : 0;
+  kern<<<static_cast<unsigned>(grid), NT, kTmaSmem, st>>>(map, a, tps, stall);
+  return cudaGetLastError();
+}
+
+} // namespace
+
+bool tma_col_ok(int L, const PassArgs &a) {
+  if (L != 256 && L != 512 && L != 1024)
+    return false;
+  if (a.batch <= 0 || a.total % a.batch != 0 || a.idist != 1)
+    return false;
+  const long long slabs = a.total / a.batch;
+  // 16-byte aligned base and strides (the tensor map's rules); x offsets are
+  // multiples of 2*TB floats (>= 64 bytes) by construction
+  if ((reinterpret_cast<uintptr_t>(a.in) & 15) != 0 || (a.istride & 1) != 0 ||
+      a.istride < a.batch)
+    return false;
+  if (slabs > 1 && ((a.islab & 1) != 0 || a.islab < a.istride * L))
+    return false;
+  if (2 * a.batch > 0xffffffffll || slabs > 0x7fffffffll || a.istride * 8 * L >= (1ll << 40) ||
+      (slabs > 1 && a.islab * 8 >= (1ll << 40)))
+    return false;
+  return encode_fn() != nullptr;
+}
+
+// FP32 column C2C pass through the TMA ring (nt = 512 or 1024 threads per
+// CTA); the caller checks tma_col_ok first.
+cudaError_t launch_tma_col_c2c_f32(int L, bool fwd, int nt, const PassArgs &a,
+                                   cudaStream_t st) {
+#define B2_TMA(LL)                                                                   \
+  case LL:                                                                           \
+    if (nt == 1024)                                                                  \
+      return fwd ? launch_tma_t<LL, 1024, true>(a, st) : launch_tma_t<LL, 1024, false>(a, st); \
+    return fwd ? launch_tma_t<LL, 512, true>(a, st) : launch_tma_t<LL, 512, false>(a, st);
+  switch (L) {
+    B2_TMA(256)
+    B2_TMA(512)
+    B2_TMA(1024)
+  default:
+    return cudaErrorInvalidValue;
+  }
+#undef B2_TMA
+}
+
+// Fault word of the TMA column kernels: returned and cleared (the stream of
+// the launches must be synchronised first).
+cudaError_t tma_take_fault(unsigned *fault) {
+  unsigned f = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&f, g_tma_fault, sizeof(f));
+  if (e != cudaSuccess)
+    return e;
+  *fault = f;
+  if (f) {
+    const unsigned zero = 0;
+    e = cudaMemcpyToSymbol(g_tma_fault, &zero, sizeof(zero));
+  }
+  return e;
+}
+
+} // namespace b200fft

@@ -49,6 +49,12 @@ cudaError_t launch_tc5_row256_f32(bool fwd, const PassArgs &a, cudaStream_t st);
 // The tcgen05 kernels' device fault word (a bounded wait that ran out),
 // returned and cleared; call after the launches' stream is synchronised.
 cudaError_t tc5_take_fault(unsigned *fault);
+// TMA-fed FP32 column C2C passes (fft_tma.cu): eligibility (lengths 256, 512,
+// 1024; contiguous transforms; 16-byte aligned base, stride and slab
+// stride), the launch (nt = 512 or 1024 threads per CTA) and the fault word.
+bool tma_col_ok(int L, const PassArgs &a);
+cudaError_t launch_tma_col_c2c_f32(int L, bool fwd, int nt, const PassArgs &a, cudaStream_t st);
+cudaError_t tma_take_fault(unsigned *fault);
 
 // Family G: runtime-generic kernels.
 cudaError_t launch_generic(bool f64, int kind, bool col, bool fwd,
