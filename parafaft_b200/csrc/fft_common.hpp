@@ -90,10 +90,21 @@ struct GenArgs {
 // the fewest stages of radices up to rmax, as even as possible, larger first
 // (1024 = 32x32 or 16x8x8, 512 = 32x16, 256 = 16x16): every stage saved is a
 // shared-memory exchange saved. Otherwise the radix order is 8s, then one 4
-// or 2, then 5s, then 3s. Returns the stage count; `rest` is what no radix
-// divides (1 for a supported length).
-constexpr int static_schedule(int L, int rmax, int (&rad)[24], int &rest) {
+// or 2, then 5s, then 3s. Rows of other lengths split over prow threads
+// (prow > 0) take the even schedule below when prow is the thread count
+// chosen for it (mixed_row_threads). Returns the stage
+// count; `rest` is what no radix divides (1 for a supported length).
+constexpr int even_row_schedule(int L, int P, int (&rad)[24]);
+constexpr int mixed_row_threads(int L);
+constexpr int static_schedule(int L, int rmax, int prow, int (&rad)[24], int &rest) {
   int k = 0;
+  if (prow > 0 && (L & (L - 1)) != 0 && mixed_row_threads(L) == prow) {
+    const int n = even_row_schedule(L, prow, rad);
+    if (n > 0) {
+      rest = 1;
+      return n;
+    }
+  }
   if (rmax > 8 && L >= 16 && (L & (L - 1)) == 0) {
     int lg = 0, q = 0;
     while ((1 << lg) < L)
@@ -131,6 +142,56 @@ constexpr int static_schedule(int L, int rmax, int (&rad)[24], int &rest) {
   return k;
 }
 
+// A row of mixed length L = 2^a 3^b 5^c over P = 2^p threads splits evenly at
+// every stage when each radix R leaves L/R a multiple of P, i.e. its
+// power-of-two radices are at most 2^(a-p) (and 8). That schedule: as few
+// power-of-two radices as that allows, as even as possible, larger first,
+// then 5s, then 3s. Every stage then fills all P threads, and R2C/C2R rows
+// pair their Hermitian halves with warp shuffles (P <= 32). Returns its stage
+// count, or 0 when there is none.
+constexpr int even_row_schedule(int L, int P, int (&rad)[24]) {
+  int a = 0, m = L, p = 0;
+  while (m % 2 == 0) {
+    m /= 2;
+    ++a;
+  }
+  while ((1 << p) < P)
+    ++p;
+  const int q = (a - p) < 3 ? (a - p) : 3;
+  if (q < 1 || (L % P) != 0)
+    return 0;
+  int k = 0;
+  const int n = (a + q - 1) / q;
+  for (int i = 0; i < n; ++i)
+    rad[k++] = 1 << (a / n + (i < a % n ? 1 : 0));
+  while (m % 5 == 0) {
+    rad[k++] = 5;
+    m /= 5;
+  }
+  while (m % 3 == 0) {
+    rad[k++] = 3;
+    m /= 3;
+  }
+  return m == 1 ? k : 0;
+}
+
+// Threads per row of a mixed-length row kernel with an even schedule: the
+// largest power of two 4 <= P <= 32 whose even schedule has at most three
+// stages and at most 24 points per thread (0: none; the kernel then takes
+// P = floor_pow2(L/8) and the default schedule). Two threads per row spread a
+// warp's loads over 16 rows, which cost more than the idle lanes it saves
+// (40-point rows: 48/52 -> 57/60 us).
+constexpr int mixed_row_threads(int L) {
+  int best = 0;
+  for (int P = 4; P <= 32; P *= 2) {
+    int rad[24] = {};
+    const int n = even_row_schedule(L, P, rad);
+    if (n > 0 && n <= 3 && L / P <= 24)
+      best = P;
+  }
+  return best;
+}
+
 // Largest radix of a specialised kernel whose threads hold E = L*TB/NT points:
 // the largest power of two <= E between 8 and 32 (16 for 16-byte elements,
 // whose 32-point butterfly would not fit the registers).
@@ -143,13 +204,13 @@ constexpr int radix_cap(int esize, int L, int TB, int NT) {
   return r;
 }
 
-template <int L, int RMAX = 8> struct SchedS {
+template <int L, int RMAX = 8, int PROW = 0> struct SchedS {
   int nst = 0;
   int rad[24] = {};
   int ns[24] = {};
   int rest = 1;
   constexpr SchedS() {
-    nst = static_schedule(L, RMAX, rad, rest);
+    nst = static_schedule(L, RMAX, PROW, rad, rest);
     int p = 1;
     for (int i = 0; i < nst; ++i) {
       ns[i] = p;
@@ -320,7 +381,8 @@ constexpr CfgS cfg_static(int esize, int L, bool col, int variant = 0) {
       const int TB = ce_min(NT, floor_pow2(ce_max(1, base / L)));
       return CfgS{NT, TB, NT / TB, (TB * L + NT - 1) / NT};
     }
-    const int P = ce_min(NT, floor_pow2(ce_max(1, L / 8)));
+    const int Pe = mixed_row_threads(L);
+    const int P = Pe > 0 ? Pe : ce_min(NT, floor_pow2(ce_max(1, L / 8)));
     return CfgS{NT, NT / P, P, (L + P - 1) / P};
   }
   const int NT = (col && (variant == 7 || variant == 9)) ? 1024
