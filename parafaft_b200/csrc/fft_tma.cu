@@ -253,7 +253,8 @@ bool tma_col_ok(int L, const PassArgs &a) {
     return false;
   if (slabs > 1 && ((a.islab & 1) != 0 || a.islab < a.istride * L))
     return false;
-  if (2 * a.batch > 0xffffffffll || slabs > 0x7fffffffll || a.istride * 8 * L >= (1ll << 40) ||
+  // tensor coordinates are signed 32-bit: the column (in floats) and the slab
+  if (2 * a.batch > 0x7fffffffll || slabs > 0x7fffffffll || a.istride * 8 * L >= (1ll << 40) ||
       (slabs > 1 && a.islab * 8 >= (1ll << 40)))
     return false;
   return encode_fn() != nullptr;
