@@ -638,6 +638,16 @@ def run_b200(args):
     st = h.stats()
     launches = st["kernel_launches"] + st["copies_issued"]
 
+    # ---- per-step distribution (a second pass, events between steps): the
+    #      median beside the mean, as the reference's GPU benchmark reports both
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(stream)
+    for i in range(args.steps):
+        step()
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    per_step = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+
     # ---- per-kernel timing (a second pass of the same steps, events around
     #      every launch on the backend's stream)
     h.set_profiling(True)
@@ -753,6 +763,8 @@ def run_b200(args):
                        "l2": "inputs larger than L2 (539 MB buffer)",
                        "replicas": world},
             "rel_l2_fwd_vs_fp64": rel_fwd, "rel_l2_roundtrip": rel_rt,
+            "step_ms_median": round(statistics.median(per_step), 4),
+            "step_ms_mean_per_step_events": round(statistics.fmean(per_step), 4),
             "hbm_roofline_frac_step": round(ALG_BYTES / (ms * 1e-3) / 1e9 / peak, 4),
             # 5 N log2 N per direction (C2C-equivalent convention), and the
             # R2C convention at half of it, labelled as such

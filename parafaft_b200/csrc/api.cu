@@ -166,6 +166,11 @@ int ilog2(int x) {
 int default_variant(int csize, int L, bool col, long long stride) {
   if (col && stride * csize >= (4ll << 20))
     return 3;
+  // columns of 2048+ points: the wide tile at any stride (its 2-8 transforms
+  // per tile still give 32-64-byte row segments; the full tile's are half
+  // that: 2048-point FP32 columns at a 1 MiB stride 2.0 -> 3.4 TB/s)
+  if (col && L >= 2048)
+    return 3;
   // FP32 columns of 1024 points: the full tile, 32 points per thread, two
   // 32-point stages
   if (col && csize == 8 && L == 1024)
