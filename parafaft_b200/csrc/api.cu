@@ -164,23 +164,28 @@ int ilog2(int x) {
 // 512 or more points use the 512-thread full tile; everything else the full
 // tile (measured on the 512^3 and 1024^3 passes).
 int default_variant(int csize, int L, bool col, long long stride) {
-  if (col && stride * csize >= (4ll << 20))
-    return 3;
-  // columns of 2048+ points: the wide tile at any stride (its 2-8 transforms
-  // per tile still give 32-64-byte row segments; the full tile's are half
-  // that: 2048-point FP32 columns at a 1 MiB stride 2.0 -> 3.4 TB/s)
-  if (col && L >= 2048)
-    return 3;
-  // FP32 columns of 1024 points: the full tile, 32 points per thread, two
-  // 32-point stages
-  if (col && csize == 8 && L == 1024)
+  if (col) {
+    // 2048+ points: the wide tile at any stride (its 2-8 transforms per tile
+    // still give 32-64-byte row segments, the full tile's half that: FP32 and
+    // FP64 2048-point columns at a 1 MiB stride 2.0 -> 3.4 TB/s)
+    if (L >= 2048)
+      return 3;
+    // 1024 points: the wide tile once point rows are 4 MiB or more apart
+    // (first axes: FP32 4.3 vs 2.9 TB/s, FP64 3.9 vs 3.0), else the full tile
+    // (FP32: 32 points per thread, two 32-point stages)
+    if (L == 1024)
+      return stride * csize >= (4ll << 20) ? 3 : 0;
+    // FP32 columns of 128-512 points: 512-thread full tiles, two CTAs per SM
+    // (at 4 MiB strides 128/256 points 6.1 TB/s vs 4.5-5.0 for the other tiles)
+    if (csize == 8 && L >= 128)
+      return 5;
+    // FP64 columns of 512 points or fewer: the full tile at any stride
+    // (256 points at a 4 MiB stride 6.4 vs 4.7 TB/s for the wide tile)
     return 0;
-  // other FP32 columns of 512+ points: 512-thread full tiles, two CTAs per SM
-  if (col && csize == 8 && L >= 512)
-    return 5;
-  // FP32 rows of 256 and 512 points: twice the points per thread (16 and 32),
-  // so the radix-16/32 schedule needs two stages instead of three
-  if (!col && csize == 8 && (L == 256 || L == 512))
+  }
+  // rows of 256 (FP32, FP64) and 512 (FP32) points: twice the points per
+  // thread, so the radix-16/32 schedule needs two stages instead of three
+  if ((L == 256 || (L == 512 && csize == 8)))
     return 1;
   return 0;
 }
