@@ -91,7 +91,8 @@ def build_drivers(force: bool = False) -> Path | None:
     src = INTEG / "parafaft_drivers.cu"
     if ref is None:
         return DRIVERS_SO if DRIVERS_SO.exists() else None
-    deps = [src, INCLUDE / "fft_backend_b200.hpp", INCLUDE / "b200fft.h",
+    deps = [src, INCLUDE / "fft_backend_b200.hpp", INCLUDE / "fft_backend_b200_grid.hpp",
+            INCLUDE / "b200fft.h",
             INTEG / "mpi_shim" / "mpi.h", ENGINE_SO]
     if force or _newer(DRIVERS_SO, deps):
         _run([_nvcc(), *NVCC_FLAGS, "-I", str(INCLUDE), "-I", str(INTEG / "mpi_shim"),

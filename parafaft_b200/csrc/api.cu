@@ -380,7 +380,10 @@ struct b200fft_handle_s {
 namespace {
 
 struct GroupStep {
-  enum { PASSES = 0, COPY = 1, COPY2D = 2, STATIC = 3 };
+  // SINGLE: a level's only pass of its (length, layout, kind, direction): it
+  // runs the plan's own kernel choice (tile variant, TMA or tensor-core form)
+  // on the group's stream rather than the grouped kernel's default tile.
+  enum { PASSES = 0, COPY = 1, COPY2D = 2, STATIC = 3, SINGLE = 4 };
   int type = PASSES;
   // grouped pass: generic kernel (PASSES, items) or specialised kernel of
   // length L (STATIC, sitems)
@@ -399,6 +402,11 @@ struct GroupStep {
   long long bytes = 0;
   // copy
   RecOp op;
+  // SINGLE (and the first item of a STATIC step)
+  b200fft_handle_s *h = nullptr;
+  Plan plan;
+  int dir = 0;
+  PassArgs pa{};
 };
 
 } // namespace
@@ -1617,6 +1625,7 @@ int group_build(G *g) {
   for (H *h : g->handles)
     depth = std::max(depth, h->recs.size());
   for (size_t d = 0; d < depth; ++d) {
+    const size_t first_step = g->steps.size();
     std::map<long long, size_t> bucket; // (static, L, f64, kind, col, fwd) -> step index
     for (H *h : g->handles) {
       if (d >= h->recs.size())
@@ -1661,6 +1670,12 @@ int group_build(G *g) {
         }
         GroupStep &s = g->steps[si];
         const PassArgs pa = pass_args(p, 0, op.in, op.out, op.tw, op.slabs, op.slab);
+        if (s.sitems.empty()) {
+          s.h = h;
+          s.plan = p;
+          s.dir = op.dir;
+          s.pa = pass_args(p, p.ch.family, op.in, op.out, op.tw, op.slabs, op.slab);
+        }
         const int tb = static_tile_transforms(h->csize(), sc.L, sc.col);
         s.sitems.push_back(pa);
         s.tile_start.push_back(s.tile_start.back() + (pa.total + tb - 1) / tb);
@@ -1697,6 +1712,9 @@ int group_build(G *g) {
       s.smem = std::max(s.smem, generic_smem_bytes(f64, ga.TB, ga.L));
       s.bytes += pass_bytes(h, p, ga.p.total);
     }
+    for (size_t i = first_step; i < g->steps.size(); ++i)
+      if (g->steps[i].type == GroupStep::STATIC && g->steps[i].sitems.size() == 1)
+        g->steps[i].type = GroupStep::SINGLE;
   }
   // device copies of the work lists, one queue counter per grouped launch
   int q = 0;
@@ -1752,7 +1770,8 @@ int group_build(G *g) {
 int group_run(G *g) {
   g->stats.exec_calls++;
   for (GroupStep &s : g->steps) {
-    if (s.type == GroupStep::PASSES || s.type == GroupStep::STATIC) {
+    if (s.type == GroupStep::PASSES || s.type == GroupStep::STATIC ||
+        s.type == GroupStep::SINGLE) {
       g->stats.kernel_launches++;
       g->stats.bytes_transformed += static_cast<uint64_t>(s.bytes);
     } else {
@@ -1790,6 +1809,9 @@ int group_run(G *g) {
                                                  s.d_tile_start, n, nt, g->stream)
                   : launch_static_group_real_f32(s.L, s.kind == KIND_R2C, s.d_sitems,
                                                  s.d_tile_start, n, nt, g->stream);
+    } else if (s.type == GroupStep::SINGLE) {
+      what = "single pass";
+      e = launch_kernel(s.h, s.plan, s.dir, s.pa);
     } else if (s.type == GroupStep::COPY) {
       what = "copy";
       e = cudaMemcpyAsync(s.op.dst, s.op.src, s.op.bytes, cudaMemcpyDefault, g->stream);

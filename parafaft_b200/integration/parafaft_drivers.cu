@@ -1,7 +1,8 @@
 // ParaFaFT's own orchestrators, ParaFaFT_C2C<D, Backend> and
 // ParaFaFT_R2C<D, Backend> (parafaft_c2c.hpp:69, parafaft_r2c.hpp:98),
-// instantiated with B200Backend<T> — the drop-in this project provides — and,
-// for comparison on the same GPU, with the reference CuFFTBackend<T>
+// instantiated with B200Backend<T> — the drop-in this project provides — and
+// B200GridBackend<D, T> (its grid-owning form), and, for comparison on the
+// same GPU, with the reference CuFFTBackend<T>
 // (backend/cufft/fft_backend_cufft.hpp). A small C ABI exposes the objects to
 // the Python tests and the benchmark, so every transform they run goes through
 // the reference's forward()/backward() code path unchanged.
@@ -26,6 +27,7 @@ template <typename FloatTypeT = double> class FFTWBackend;
 
 #include "b200fft.h"
 #include "fft_backend_b200.hpp"
+#include "fft_backend_b200_grid.hpp"
 
 namespace {
 
@@ -39,6 +41,8 @@ struct Obj {
   virtual void backward_oop(void *in, void *out) = 0;
   virtual long long required_size() const = 0;
   virtual void shapes(int *in_shape, int *in_start, int *out_shape, int *out_start) const = 0;
+  // the backend-owned grid buffer (backends with handles_distributed), else null
+  virtual void *buffer() { return nullptr; }
   int ndim = 0;
   bool r2c = false;
   b200fft_handle handle = nullptr;
@@ -65,6 +69,7 @@ template <int D, class B> struct C2CObj : Obj {
   long long required_size() const override {
     return static_cast<long long>(f->get_required_output_size());
   }
+  void *buffer() override { return f->get_buffer(); }
   void shapes(int *a, int *b, int *c, int *d) const override {
     f->get_local_shape(a);
     f->get_global_start(b);
@@ -96,6 +101,7 @@ template <int D, class B> struct R2CObj : Obj {
   long long required_size() const override {
     return static_cast<long long>(f->get_required_output_size());
   }
+  void *buffer() override { return f->get_real_buffer(); }
   void shapes(int *a, int *b, int *c, int *d) const override {
     f->get_local_real_shape(a);
     f->get_real_global_start(b);
@@ -222,6 +228,25 @@ Obj *make(int D, int prec, int backend, const int *shape, int plan_flag) {
   throw std::runtime_error("backend must be 0 (B200Backend) or 1 (CuFFTBackend)");
 }
 
+// ParaFaFT objects on B200GridBackend<D, T> (the grid-owning backend; the
+// reference orchestrators only, whose distributed path takes any shape).
+template <template <int, class> class O, class T>
+Obj *make_grid_t(int D, const int *shape, parafaft::FFTPlanFlag flag) {
+  switch (D) {
+  case 2: return new O<2, parafaft::B200GridBackend<2, T>>(shape, flag);
+  case 3: return new O<3, parafaft::B200GridBackend<3, T>>(shape, flag);
+  case 4: return new O<4, parafaft::B200GridBackend<4, T>>(shape, flag);
+  case 5: return new O<5, parafaft::B200GridBackend<5, T>>(shape, flag);
+  default: throw std::runtime_error("D must be 2..5");
+  }
+}
+template <template <int, class> class O>
+Obj *make_grid(int D, int prec, const int *shape, int plan_flag) {
+  const auto flag = static_cast<parafaft::FFTPlanFlag>(plan_flag);
+  return prec == B200FFT_F64 ? make_grid_t<O, double>(D, shape, flag)
+                             : make_grid_t<O, float>(D, shape, flag);
+}
+
 template <class F> int guard(F f) {
   try {
     f();
@@ -243,14 +268,21 @@ const char *pfb_last_error(void) { return g_err.c_str(); }
 
 // kind: 0 C2C (ParaFaFT_C2C), 1 R2C (ParaFaFT_R2C), 2 C2C through the
 // one-rank orchestrator above (any grid shape). backend: 0 B200Backend,
-// 1 CuFFTBackend. prec: B200FFT_F32/F64.
+// 1 CuFFTBackend, 2 B200GridBackend (the grid-owning backend: kinds 0 and 1;
+// forward/backward then ignore their data argument and transform the buffer
+// pfb_buffer returns). prec: B200FFT_F32/F64.
 int pfb_create(int kind, int D, int prec, int backend, const int *shape, int plan_flag,
                void **out) {
   return guard([&] {
     *out = nullptr;
-    Obj *o = kind == 0   ? make<C2CObj>(D, prec, backend, shape, plan_flag)
-             : kind == 1 ? make<R2CObj>(D, prec, backend, shape, plan_flag)
-                         : make<OneRankC2C>(D, prec, backend, shape, plan_flag);
+    if (backend == 2 && kind == 2)
+      throw std::runtime_error("the grid-owning backend runs through the reference "
+                               "orchestrators (kind c2c or r2c)");
+    Obj *o = backend == 2 ? (kind == 0 ? make_grid<C2CObj>(D, prec, shape, plan_flag)
+                                       : make_grid<R2CObj>(D, prec, shape, plan_flag))
+             : kind == 0  ? make<C2CObj>(D, prec, backend, shape, plan_flag)
+             : kind == 1  ? make<R2CObj>(D, prec, backend, shape, plan_flag)
+                          : make<OneRankC2C>(D, prec, backend, shape, plan_flag);
     *out = o;
   });
 }
@@ -283,5 +315,7 @@ int pfb_shapes(void *h, int *in_shape, int *in_start, int *out_shape, int *out_s
 
 // The B200 handle inside the object (null for CuFFTBackend objects).
 void *pfb_b200_handle(void *h) { return static_cast<Obj *>(h)->handle; }
+// Device pointer of the grid a grid-owning backend holds (null otherwise).
+void *pfb_buffer(void *h) { return static_cast<Obj *>(h)->buffer(); }
 
 } // extern "C"

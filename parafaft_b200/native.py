@@ -156,6 +156,7 @@ def drivers() -> C.CDLL:
             ("pfb_required_size", C.c_longlong, [vp]),
             ("pfb_shapes", i, [vp, ip, ip, ip, ip]),
             ("pfb_b200_handle", vp, [vp]),
+            ("pfb_buffer", vp, [vp]),
         ):
             fn = getattr(lib, name)
             fn.restype = res
@@ -368,9 +369,11 @@ class ParaFaFT:
 
     kind: "c2c" or "r2c" (the reference orchestrators), or "c2c_onerank" (the
     same backend call sequence with per-axis extents, for grids that are not
-    hypercubic); backend: "b200" (B200Backend<T>) or "cufft"
-    (the reference CuFFTBackend<T>, for comparison). Data arguments are device
-    pointers (ints) or CUDA torch tensors.
+    hypercubic); backend: "b200" (B200Backend<T>), "b200grid"
+    (B200GridBackend<D, T>, which owns the grid: forward/backward transform
+    the buffer() it holds and ignore their argument) or "cufft" (the reference
+    CuFFTBackend<T>, for comparison). Data arguments are device pointers (ints)
+    or CUDA torch tensors.
     """
 
     def __init__(self, kind: str, shape, precision: int = F32, backend: str = "b200",
@@ -383,8 +386,9 @@ class ParaFaFT:
         arr = (C.c_int * self.D)(*self.shape)
         h = C.c_void_p()
         kinds = {"c2c": 0, "r2c": 1, "c2c_onerank": 2}
-        rc = self._lib.pfb_create(kinds[kind], self.D, precision,
-                                  0 if backend == "b200" else 1, arr, plan_flag, C.byref(h))
+        backends = {"b200": 0, "cufft": 1, "b200grid": 2}
+        rc = self._lib.pfb_create(kinds[kind], self.D, precision, backends[backend], arr,
+                                  plan_flag, C.byref(h))
         if rc != 0:
             raise RuntimeError("ParaFaFT construction failed: " + self._lib.pfb_last_error().decode())
         self._h = h
@@ -428,6 +432,28 @@ class ParaFaFT:
         self._check(self._lib.pfb_shapes(self._h, a, b, c, d))
         return {"in_shape": list(a), "in_start": list(b), "out_shape": list(c),
                 "out_start": list(d)}
+
+    def buffer(self):
+        """The grid a grid-owning backend holds, as a CUDA torch tensor viewing
+        it (complex for C2C, the padded reals for R2C), or None."""
+        import torch
+        raw = self._lib.pfb_buffer(self._h)
+        if not raw:
+            return None
+        n = self.shape[-1]
+        rows = 1
+        for s in self.shape[:-1]:
+            rows *= s
+        f64 = self.precision == F64
+        if self.kind == "r2c":
+            count, typestr = rows * 2 * (n // 2 + 1), "<f8" if f64 else "<f4"
+        else:
+            count, typestr = rows * n, "<c16" if f64 else "<c8"
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (count,), "typestr": typestr,
+                                        "data": (int(raw), False), "version": 2}
+        return torch.as_tensor(_View(), device="cuda")
 
     def handle(self) -> Handle | None:
         raw = self._lib.pfb_b200_handle(self._h)
