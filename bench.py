@@ -414,9 +414,62 @@ def run_c2c_config(args):
         "gpu_launches_per_step": st["kernel_launches"] / args.steps,
         "copies_issued_per_step": st["copies_issued"] / args.steps,
     }
-    print(json.dumps(line), flush=True)
     f.close()
+    if args.form == "plain":
+        # fresh input (the timing loop above left unnormalised round trips in data)
+        del data
+        torch.cuda.empty_cache()
+        gen2 = torch.Generator(device="cuda").manual_seed(seed + 1)
+        line["grid_backend"] = time_grid_backend(
+            "c2c", shape, prec,
+            lambda b: b.copy_(torch.randn(b.numel(), generator=gen2, device="cuda", dtype=b.dtype)),
+            args.steps, args.warmup)
+        line["grid_backend"]["hbm_frac"] = round(
+            alg / (line["grid_backend"]["ms"] * 1e-3) / 1e9 / peak, 4)
+    print(json.dumps(line), flush=True)
     return 0
+
+
+def time_grid_backend(kind, shape, prec, fill, steps, warmup):
+    """The same forward+backward through the reference orchestrator on
+    B200GridBackend<D, T> (the grid-owning backend: each transform one
+    replayed CUDA graph on the backend's own buffer). `fill(buf)` writes the
+    input into that buffer. Returns ms per step (CUDA events; forward and
+    backward wait for their graph), the round-trip rel-L2 and launches per step."""
+    import torch
+    from parafaft_b200 import native as nv
+    g = nv.ParaFaFT(kind, shape, prec, backend="b200grid")
+    buf = g.buffer()
+    fill(buf)
+    x0 = buf.clone()
+    n = int(np.prod(shape))
+    g.forward(None)
+    g.backward(None)
+    if kind == "r2c":
+        ref = x0.view(-1, 2 * (shape[-1] // 2 + 1))[:, :shape[-1]].double()
+        got = buf.view(-1, 2 * (shape[-1] // 2 + 1))[:, :shape[-1]].double() / n
+    else:
+        ref, got = x0.to(torch.complex128), buf.to(torch.complex128) / n
+    rt = float(torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref))
+    del ref, got, x0
+    for _ in range(warmup):
+        g.forward(None)
+        g.backward(None)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        g.forward(None)
+        g.backward(None)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    g.close()
+    torch.cuda.empty_cache()
+    return {"ms": round(ms, 4), "rel_l2_roundtrip": rt,
+            "backend": f"ParaFaFT_{'R2C' if kind == 'r2c' else 'C2C'}<{len(shape)}, "
+                       f"B200GridBackend<{len(shape)}, {'double' if prec == nv.F64 else 'float'}>>"}
 
 
 UNEVEN_SIDES = [32, 48, 60, 64, 80, 96, 120, 128, 160]
@@ -723,6 +776,11 @@ def run_b200(args):
     #      column passes (512-point C2C) on the tensor cores, FP16 hi+lo
     split = measure_split_tc(args, pinned, x_real, dev, stream, ms)
 
+    # ---- the same step through the grid-owning backend (handles_distributed)
+    grid = time_grid_backend("r2c", SHAPE, nv.F32, lambda b: b.copy_(pinned[:b.numel()]),
+                             args.steps, args.warmup)
+    grid["hbm_frac"] = round(ALG_BYTES / (grid["ms"] * 1e-3) / 1e9 / _peaks()[0], 4)
+
     # ---- the reference's cuFFT backend on the same GPU, same orchestrator
     cufft_ms = None
     try:
@@ -780,6 +838,7 @@ def run_b200(args):
                     "pipeline": "three device buffers; step i+1's upload, step i's transform and step i-1's download overlap"},
             "cufft_backend_ms": cufft_ms if isinstance(cufft_ms, str) else round(cufft_ms, 4),
             "split_tc": split,
+            "grid_backend": grid,
             "gpu_launches": int(launches),
             "clocks": clk,
             "cpu_baseline": {"value": round(cpu_ms, 1), "unit": "ms", "cores": cores, "kind": "port",
