@@ -402,6 +402,7 @@ struct GroupStep {
   long long bytes = 0;
   // copy
   RecOp op;
+  int level = 0; // dependency level (the level's steps are independent)
   // SINGLE (and the first item of a STATIC step)
   b200fft_handle_s *h = nullptr;
   Plan plan;
@@ -410,6 +411,9 @@ struct GroupStep {
 };
 
 } // namespace
+
+// Streams a level of a group schedule spreads its independent steps over.
+constexpr int kGroupStreams = 8;
 
 struct b200fft_group_s {
   std::vector<b200fft_handle_s *> handles;
@@ -422,6 +426,12 @@ struct b200fft_group_s {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   b200fft_stats stats{};
+  // the steps of one level run side by side: step i of a level on
+  // streams[i % size] (streams[0] is the group's stream), forked from and
+  // joined back into the group's stream by events around the level
+  std::vector<cudaStream_t> aux;
+  std::vector<cudaEvent_t> aux_done;
+  cudaEvent_t level_start = nullptr;
 };
 
 namespace {
@@ -1602,7 +1612,16 @@ void group_free_schedule(G *g) {
     }
     if (g->d_queues)
       cudaFree(g->d_queues);
+    for (cudaStream_t s : g->aux)
+      cudaStreamDestroy(s);
+    for (cudaEvent_t e : g->aux_done)
+      cudaEventDestroy(e);
+    if (g->level_start)
+      cudaEventDestroy(g->level_start);
   }
+  g->aux.clear();
+  g->aux_done.clear();
+  g->level_start = nullptr;
   g->d_queues = nullptr;
   g->nqueues = 0;
   g->steps.clear();
@@ -1712,9 +1731,36 @@ int group_build(G *g) {
       s.smem = std::max(s.smem, generic_smem_bytes(f64, ga.TB, ga.L));
       s.bytes += pass_bytes(h, p, ga.p.total);
     }
-    for (size_t i = first_step; i < g->steps.size(); ++i)
+    for (size_t i = first_step; i < g->steps.size(); ++i) {
+      g->steps[i].level = static_cast<int>(d);
       if (g->steps[i].type == GroupStep::STATIC && g->steps[i].sitems.size() == 1)
         g->steps[i].type = GroupStep::SINGLE;
+    }
+  }
+  // streams for the widest level (at most kGroupStreams side by side)
+  if (!g->record_only) {
+    size_t widest = 1, run = 0;
+    for (size_t i = 0; i < g->steps.size(); ++i) {
+      run = (i > 0 && g->steps[i].level == g->steps[i - 1].level) ? run + 1 : 1;
+      widest = std::max(widest, run);
+    }
+    const size_t naux = std::min(widest, static_cast<size_t>(kGroupStreams)) - 1;
+    if (naux > 0) {
+      cudaError_t e = cudaEventCreateWithFlags(&g->level_start, cudaEventDisableTiming);
+      for (size_t k = 0; k < naux && e == cudaSuccess; ++k) {
+        cudaStream_t s = nullptr;
+        e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        if (e == cudaSuccess)
+          g->aux.push_back(s);
+        cudaEvent_t ev = nullptr;
+        if (e == cudaSuccess)
+          e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess)
+          g->aux_done.push_back(ev);
+      }
+      if (e != cudaSuccess)
+        return cuda_fail(e, "group streams");
+    }
   }
   // device copies of the work lists, one queue counter per grouped launch
   int q = 0;
@@ -1781,51 +1827,81 @@ int group_run(G *g) {
   if (g->record_only)
     return B200FFT_SUCCESS;
   cudaGetLastError(); // report only errors of the calls below
-  for (size_t i = 0; i < g->steps.size(); ++i) {
-    GroupStep &s = g->steps[i];
-    cudaError_t e = cudaSuccess;
-    const char *what = "grouped pass";
-    if (s.type == GroupStep::PASSES) {
-      if (s.tile_start.back() == 0)
-        continue;
-      e = cudaMemsetAsync(g->d_queues + s.queue, 0, sizeof(unsigned long long), g->stream);
+  const size_t nstreams = 1 + g->aux.size();
+  for (size_t lv = 0; lv < g->steps.size();) {
+    size_t lv_end = lv;
+    while (lv_end < g->steps.size() && g->steps[lv_end].level == g->steps[lv].level)
+      ++lv_end;
+    const size_t width = std::min(lv_end - lv, nstreams);
+    if (width > 1) { // fork: the level's other streams start after the previous level
+      cudaError_t e = cudaEventRecord(g->level_start, g->stream);
+      for (size_t k = 1; k < width && e == cudaSuccess; ++k)
+        e = cudaStreamWaitEvent(g->aux[k - 1], g->level_start, 0);
       if (e != cudaSuccess)
-        what = "queue reset";
-      else
-        e = launch_generic_group(s.f64, s.kind, s.col, s.fwd, s.d_items, s.d_tile_start,
-                                 static_cast<int>(s.items.size()), g->d_queues + s.queue,
-                                 s.smem, s.grid, g->stream);
-    } else if (s.type == GroupStep::STATIC) {
-      what = "grouped specialised pass";
-      const int n = static_cast<int>(s.sitems.size());
-      const long long nt = s.tile_start.back();
-      if (s.kind == KIND_C2C)
-        e = s.f64 ? launch_static_group_c2c_f64(s.L, s.col, s.fwd, s.d_sitems, s.d_tile_start, n,
-                                                nt, g->stream)
-                  : launch_static_group_c2c_f32(s.L, s.col, s.fwd, s.d_sitems, s.d_tile_start, n,
-                                                nt, g->stream);
-      else
-        e = s.f64 ? launch_static_group_real_f64(s.L, s.kind == KIND_R2C, s.d_sitems,
-                                                 s.d_tile_start, n, nt, g->stream)
-                  : launch_static_group_real_f32(s.L, s.kind == KIND_R2C, s.d_sitems,
-                                                 s.d_tile_start, n, nt, g->stream);
-    } else if (s.type == GroupStep::SINGLE) {
-      what = "single pass";
-      e = launch_kernel(s.h, s.plan, s.dir, s.pa);
-    } else if (s.type == GroupStep::COPY) {
-      what = "copy";
-      e = cudaMemcpyAsync(s.op.dst, s.op.src, s.op.bytes, cudaMemcpyDefault, g->stream);
-    } else {
-      what = "2D copy";
-      e = cudaMemcpy2DAsync(s.op.dst, s.op.dpitch, s.op.src, s.op.spitch, s.op.width,
-                            s.op.height, cudaMemcpyDefault, g->stream);
+        return cuda_fail(e, "group level fork");
     }
-    if (e != cudaSuccess) {
-      char buf[160];
-      std::snprintf(buf, sizeof(buf), "group step %zu (%s, kind %d, %zu items, grid %d, smem %zu)",
-                    i, what, s.kind, s.items.size(), s.grid, s.smem);
-      return cuda_fail(e, buf);
+    for (size_t i = lv; i < lv_end; ++i) {
+      GroupStep &s = g->steps[i];
+      const size_t lane = (i - lv) % nstreams;
+      cudaStream_t st = lane == 0 ? g->stream : g->aux[lane - 1];
+      cudaError_t e = cudaSuccess;
+      const char *what = "grouped pass";
+      if (s.type == GroupStep::PASSES) {
+        if (s.tile_start.back() == 0)
+          continue;
+        e = cudaMemsetAsync(g->d_queues + s.queue, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess)
+          what = "queue reset";
+        else
+          e = launch_generic_group(s.f64, s.kind, s.col, s.fwd, s.d_items, s.d_tile_start,
+                                   static_cast<int>(s.items.size()), g->d_queues + s.queue,
+                                   s.smem, s.grid, st);
+      } else if (s.type == GroupStep::STATIC) {
+        what = "grouped specialised pass";
+        const int n = static_cast<int>(s.sitems.size());
+        const long long nt = s.tile_start.back();
+        if (s.kind == KIND_C2C)
+          e = s.f64 ? launch_static_group_c2c_f64(s.L, s.col, s.fwd, s.d_sitems, s.d_tile_start, n,
+                                                  nt, st)
+                    : launch_static_group_c2c_f32(s.L, s.col, s.fwd, s.d_sitems, s.d_tile_start, n,
+                                                  nt, st);
+        else
+          e = s.f64 ? launch_static_group_real_f64(s.L, s.kind == KIND_R2C, s.d_sitems,
+                                                   s.d_tile_start, n, nt, st)
+                    : launch_static_group_real_f32(s.L, s.kind == KIND_R2C, s.d_sitems,
+                                                   s.d_tile_start, n, nt, st);
+      } else if (s.type == GroupStep::SINGLE) {
+        what = "single pass";
+        cudaStream_t keep = s.h->stream;
+        s.h->stream = st; // the plan's launch goes to this step's stream
+        e = launch_kernel(s.h, s.plan, s.dir, s.pa);
+        s.h->stream = keep;
+      } else if (s.type == GroupStep::COPY) {
+        what = "copy";
+        e = cudaMemcpyAsync(s.op.dst, s.op.src, s.op.bytes, cudaMemcpyDefault, st);
+      } else {
+        what = "2D copy";
+        e = cudaMemcpy2DAsync(s.op.dst, s.op.dpitch, s.op.src, s.op.spitch, s.op.width,
+                              s.op.height, cudaMemcpyDefault, st);
+      }
+      if (e != cudaSuccess) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "group step %zu (%s, kind %d, %zu items, grid %d, smem %zu)",
+                      i, what, s.kind, s.items.size(), s.grid, s.smem);
+        return cuda_fail(e, buf);
+      }
     }
+    if (width > 1) { // join: the next level starts after all of this one
+      cudaError_t e = cudaSuccess;
+      for (size_t k = 1; k < width && e == cudaSuccess; ++k) {
+        e = cudaEventRecord(g->aux_done[k - 1], g->aux[k - 1]);
+        if (e == cudaSuccess)
+          e = cudaStreamWaitEvent(g->stream, g->aux_done[k - 1], 0);
+      }
+      if (e != cudaSuccess)
+        return cuda_fail(e, "group level join");
+    }
+    lv = lv_end;
   }
   return B200FFT_SUCCESS;
 }
