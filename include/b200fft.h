@@ -184,11 +184,15 @@ int b200fft_free(void *ptr);
  * b200fft_group_begin and b200fft_group_end their passes are recorded (after
  * the usual copy fusion and slice coalescing) instead of launched, and
  * b200fft_sync on them returns at once. b200fft_group_end then runs the
- * recording: the d-th recorded pass of every handle forms one persistent
+ * recording level by level (level d: the d-th recorded pass or copy of every
+ * handle): passes with a specialised kernel launch once per (precision, kind,
+ * layout, direction, length), one CTA per tile of any handle's pass (a single
+ * pass launches its plan's own kernel); the others share one persistent
  * launch whose CTAs take (transform, tile) work items from a device queue.
- * The recorded schedule stays valid for the same buffers: group_replay runs
- * it again, group_capture records it once into a CUDA graph that replay then
- * launches. */
+ * The launches of one level run side by side on several streams, so the
+ * handles of a group must not share data. The recorded schedule stays valid
+ * for the same buffers: group_replay runs it again, group_capture records it
+ * once into a CUDA graph that replay then launches. */
 typedef struct b200fft_group_s *b200fft_group;
 int b200fft_group_create(b200fft_group *out);
 /* Detaches the member handles (they return to their own streams). */
