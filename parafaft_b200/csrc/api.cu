@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -757,18 +758,18 @@ int launch_pass(H *h, const Plan &p, int dir, const void *in, void *out,
 
 // The kernel launch of one pass (no bookkeeping).
 int device_sms(int dev) {
-  static int n[32] = {0};
+  static std::atomic<int> n[32] = {}; // per device; every thread stores the same value
   if (dev < 0 || dev >= 32)
     return 148;
-  if (n[dev] == 0) {
-    int v = 0;
+  int v = n[dev].load();
+  if (v == 0) {
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
       cudaGetLastError();
       v = 148;
     }
-    n[dev] = v;
+    n[dev].store(v);
   }
-  return n[dev];
+  return v;
 }
 
 // Tile of a specialised column pass at launch: a pass too small to give every

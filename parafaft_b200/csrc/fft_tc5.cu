@@ -32,6 +32,7 @@
 
 #include <stdint.h>
 #include <cstdio>
+#include <atomic>
 #include <cstdlib>
 
 #include "fft_device.cuh"
@@ -363,7 +364,7 @@ cudaError_t launch_tc5_row256_f32(bool fwd, const PassArgs &a, cudaStream_t st) 
   const long long ntiles = (a.total + kTc5TB - 1) / kTc5TB;
   if (ntiles <= 0)
     return cudaSuccess;
-  static int per_sm[32] = {0};
+  static std::atomic<int> per_sm[32] = {}; // per device; every thread stores the same value
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 32)

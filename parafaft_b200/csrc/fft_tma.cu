@@ -23,6 +23,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdlib>
 #include <mutex>
@@ -197,15 +198,15 @@ cudaError_t launch_tma_t(const PassArgs &a, cudaStream_t st) {
   constexpr int TB = kTmaTileBytes / (L * 8);
   constexpr int ROWS = L < kTmaMaxRows ? L : kTmaMaxRows;
   auto kern = fft_tma_col_kernel<L, NT, FWD>;
-  static int configured_mask = 0;
+  static std::atomic<int> configured_mask{0}; // devices opted in
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 31 && !(configured_mask & (1 << dev))) {
+  if (dev >= 0 && dev < 31 && !(configured_mask.load() & (1 << dev))) {
     cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem);
     if (e != cudaSuccess)
       return e;
-    configured_mask |= (1 << dev);
+    configured_mask.fetch_or(1 << dev);
   }
   PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
   if (enc == nullptr)

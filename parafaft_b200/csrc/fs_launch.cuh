@@ -3,6 +3,7 @@
 // and kind, so the kernel set compiles in parallel.
 #pragma once
 
+#include <atomic>
 #include <climits>
 
 #include "fft_device.cuh"
@@ -18,15 +19,15 @@ cudaError_t launch_static_one(const PassArgs &a, cudaStream_t st) {
   constexpr size_t smem = K::smem_bytes();
   if constexpr (smem > 48 * 1024) {
     // The opt-in is per device; setting it again is cheap and idempotent.
-    static int configured_mask = 0;
+    static std::atomic<int> configured_mask{0}; // devices opted in
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 31 && !(configured_mask & (1 << dev))) {
+    if (dev >= 0 && dev < 31 && !(configured_mask.load() & (1 << dev))) {
       cudaError_t e = cudaFuncSetAttribute(
           kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
       if (e != cudaSuccess)
         return e;
-      configured_mask |= (1 << dev);
+      configured_mask.fetch_or(1 << dev);
     }
   }
   const long long grid = (a.total + cf.TB - 1) / cf.TB;
@@ -39,18 +40,18 @@ cudaError_t launch_static_one(const PassArgs &a, cudaStream_t st) {
 }
 
 inline int sm_count() {
-  static int n[32] = {0};
+  static std::atomic<int> n[32] = {}; // per device; every thread stores the same value
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 32)
     dev = 0;
-  if (n[dev] == 0) {
-    int v = 0;
+  int v = n[dev].load();
+  if (v == 0) {
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
       v = 148;
-    n[dev] = v;
+    n[dev].store(v);
   }
-  return n[dev];
+  return v;
 }
 
 template <typename T, int L, bool FWD>
@@ -59,15 +60,15 @@ cudaError_t launch_static_staged(const PassArgs &a, cudaStream_t st) {
   using K = KS<T, L, cf.NT, cf.TB, true, FWD, KIND_C2C, true>;
   auto kern = fft_static_staged_kernel<T, L, cf.NT, cf.TB, FWD>;
   constexpr size_t smem = K::smem_bytes();
-  static int configured_mask = 0;
+  static std::atomic<int> configured_mask{0}; // devices opted in
   int dev = 0;
   cudaGetDevice(&dev);
-  if (smem > 48 * 1024 && dev >= 0 && dev < 31 && !(configured_mask & (1 << dev))) {
+  if (smem > 48 * 1024 && dev >= 0 && dev < 31 && !(configured_mask.load() & (1 << dev))) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess)
       return e;
-    configured_mask |= (1 << dev);
+    configured_mask.fetch_or(1 << dev);
   }
   const long long ntiles = (a.total + cf.TB - 1) / cf.TB;
   if (ntiles <= 0)
@@ -86,15 +87,15 @@ cudaError_t launch_static_pipelined(const PassArgs &a, cudaStream_t st) {
   using K = KS<T, L, cf.NT, cf.TB, true, FWD, KIND_C2C>;
   auto kern = fft_static_pipelined_kernel<T, L, cf.NT, cf.TB, FWD>;
   constexpr size_t smem = 2 * K::smem_bytes();
-  static int configured_mask = 0;
+  static std::atomic<int> configured_mask{0}; // devices opted in
   int dev = 0;
   cudaGetDevice(&dev);
-  if (smem > 48 * 1024 && dev >= 0 && dev < 31 && !(configured_mask & (1 << dev))) {
+  if (smem > 48 * 1024 && dev >= 0 && dev < 31 && !(configured_mask.load() & (1 << dev))) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess)
       return e;
-    configured_mask |= (1 << dev);
+    configured_mask.fetch_or(1 << dev);
   }
   const long long ntiles = (a.total + cf.TB - 1) / cf.TB;
   if (ntiles <= 0)
@@ -146,15 +147,15 @@ cudaError_t launch_static_group_one(const PassArgs *items, const long long *tile
   auto kern = fft_static_group_kernel<T, L, cf.NT, cf.TB, COL, FWD, KIND>;
   constexpr size_t smem = K::smem_bytes();
   if constexpr (smem > 48 * 1024) {
-    static int configured_mask = 0;
+    static std::atomic<int> configured_mask{0}; // devices opted in
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 31 && !(configured_mask & (1 << dev))) {
+    if (dev >= 0 && dev < 31 && !(configured_mask.load() & (1 << dev))) {
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(smem));
       if (e != cudaSuccess)
         return e;
-      configured_mask |= (1 << dev);
+      configured_mask.fetch_or(1 << dev);
     }
   }
   if (ntiles <= 0)
