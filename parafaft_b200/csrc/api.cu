@@ -303,7 +303,8 @@ std::string describe_choice(const Choice &ch, int kind) {
   } else if (ch.family == 0) {
     int r[24] = {}, rest = 1;
     const int n = static_schedule(ch.L, radix_cap(ch.esize, ch.L, ch.TB, ch.NT),
-                                  ch.col ? 0 : ch.NT / ch.TB, r, rest);
+                                  ch.col ? 0 : even_row_threads(ch.L, ch.esize, ch.NT / ch.TB),
+                                  r, rest);
     for (int i = 0; i < n; ++i)
       rad += (i ? "x" : "") + std::to_string(r[i]);
   } else {

@@ -90,15 +90,14 @@ struct GenArgs {
 // the fewest stages of radices up to rmax, as even as possible, larger first
 // (1024 = 32x32 or 16x8x8, 512 = 32x16, 256 = 16x16): every stage saved is a
 // shared-memory exchange saved. Otherwise the radix order is 8s, then one 4
-// or 2, then 5s, then 3s. Rows of other lengths split over prow threads
-// (prow > 0) take the even schedule below when prow is the thread count
-// chosen for it (mixed_row_threads). Returns the stage
-// count; `rest` is what no radix divides (1 for a supported length).
+// or 2, then 5s, then 3s. Rows of other lengths given prow > 0 (the thread
+// count mixed_row_threads chose for them) take the even schedule below.
+// Returns the stage count; `rest` is what no radix divides (1 for a
+// supported length).
 constexpr int even_row_schedule(int L, int P, int (&rad)[24]);
-constexpr int mixed_row_threads(int L);
 constexpr int static_schedule(int L, int rmax, int prow, int (&rad)[24], int &rest) {
   int k = 0;
-  if (prow > 0 && (L & (L - 1)) != 0 && mixed_row_threads(L) == prow) {
+  if (prow > 0 && (L & (L - 1)) != 0) {
     const int n = even_row_schedule(L, prow, rad);
     if (n > 0) {
       rest = 1;
@@ -177,19 +176,26 @@ constexpr int even_row_schedule(int L, int P, int (&rad)[24]) {
 
 // Threads per row of a mixed-length row kernel with an even schedule: the
 // largest power of two 4 <= P <= 32 whose even schedule has at most three
-// stages and at most 24 points per thread (0: none; the kernel then takes
-// P = floor_pow2(L/8) and the default schedule). Two threads per row spread a
-// warp's loads over 16 rows, which cost more than the idle lanes it saves
-// (40-point rows: 48/52 -> 57/60 us).
-constexpr int mixed_row_threads(int L) {
+// stages and at most 24 (8-byte elements) / 12 (16-byte elements, whose
+// registers fill twice as fast) points per thread; 0: none, the kernel then
+// takes P = floor_pow2(L/8) and the default schedule. Two threads per row
+// spread a warp's loads over 16 rows, which cost more than the idle lanes it
+// saves (40-point rows: 48/52 -> 57/60 us).
+constexpr int mixed_row_threads(int L, int esize) {
   int best = 0;
   for (int P = 4; P <= 32; P *= 2) {
     int rad[24] = {};
     const int n = even_row_schedule(L, P, rad);
-    if (n > 0 && n <= 3 && L / P <= 24)
+    if (n > 0 && n <= 3 && L / P <= (esize == 8 ? 24 : 12))
       best = P;
   }
   return best;
+}
+
+// The prow argument of static_schedule for a row kernel of P threads per
+// transform: P when that is the even-schedule thread count, else 0.
+constexpr int even_row_threads(int L, int esize, int P) {
+  return ((L & (L - 1)) != 0 && mixed_row_threads(L, esize) == P) ? P : 0;
 }
 
 // Largest radix of a specialised kernel whose threads hold E = L*TB/NT points:
@@ -381,7 +387,7 @@ constexpr CfgS cfg_static(int esize, int L, bool col, int variant = 0) {
       const int TB = ce_min(NT, floor_pow2(ce_max(1, base / L)));
       return CfgS{NT, TB, NT / TB, (TB * L + NT - 1) / NT};
     }
-    const int Pe = mixed_row_threads(L);
+    const int Pe = mixed_row_threads(L, esize);
     const int P = Pe > 0 ? Pe : ce_min(NT, floor_pow2(ce_max(1, L / 8)));
     return CfgS{NT, NT / P, P, (L + P - 1) / P};
   }

@@ -368,7 +368,9 @@ template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND,
 struct KS {
   using V = cvec<T>;
   // radices up to the points a thread holds (32 / 16 at most)
-  static constexpr SchedS<L, radix_cap(int(sizeof(V)), L, TB, NT), COL ? 0 : NT / TB> S{};
+  static constexpr SchedS<L, radix_cap(int(sizeof(V)), L, TB, NT),
+                          COL ? 0 : even_row_threads(L, int(sizeof(V)), NT / TB)>
+      S{};
   static constexpr int NST = S.nst;
   static constexpr int P = NT / TB; // threads per transform
   static constexpr int TSCALE = (KIND == KIND_C2C) ? 1 : 2;
