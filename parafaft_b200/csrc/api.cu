@@ -165,6 +165,11 @@ int ilog2(int x) {
 // 512 or more points use the 512-thread full tile; everything else the full
 // tile (measured on the 512^3 and 1024^3 passes).
 int default_variant(int csize, int L, bool col, long long stride) {
+  if (col && !is_pow2(L))
+    // FP32 mixed-length columns of up to 256 points: the half tile (still >= 16
+    // transforms; 60/80/120/160 points 6-12% faster as single plans; grouped
+    // launches keep the full tile, where the half tile was slower)
+    return (csize == 8 && L <= 256) ? 1 : 0;
   if (col) {
     // 2048+ points: the wide tile at any stride (its 2-8 transforms per tile
     // still give 32-64-byte row segments, the full tile's half that: FP32 and
@@ -240,8 +245,8 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
         var = v[0] - '0';
     if (variant >= 0 && variant < kStaticVariants)
       var = variant;
-    if (!is_pow2(L))
-      var = 0; // mixed-radix lengths have the full tile only
+    if (!is_pow2(L) && !(ch.col && var == 1))
+      var = 0; // mixed-radix lengths: the full tile, or the half tile for columns
     const CfgS c = cfg_static(csize, L, ch.col, var);
     ch.variant = var;
     ch.family = 0;

@@ -379,12 +379,14 @@ constexpr int floor_pow2(int x) {
 
 constexpr CfgS cfg_static(int esize, int L, bool col, int variant = 0) {
   if (!is_pow2(L)) {
-    // Mixed-radix lengths (factors 8, 4, 2, 5, 3): the full tile only, with
-    // power-of-two tiles and thread counts per transform.
+    // Mixed-radix lengths (factors 8, 4, 2, 5, 3): power-of-two tiles and
+    // thread counts per transform; columns also take the half tile (variant
+    // 1: 10-15 points per thread, more CTAs per SM).
     const int NT = 256;
     const int base = esize == 8 ? 8192 : 4096;
     if (col) {
-      const int TB = ce_min(NT, floor_pow2(ce_max(1, base / L)));
+      const int tile = base >> (variant == 1 ? 1 : 0);
+      const int TB = ce_min(NT, floor_pow2(ce_max(1, tile / L)));
       return CfgS{NT, TB, NT / TB, (TB * L + NT - 1) / NT};
     }
     const int Pe = mixed_row_threads(L, esize);

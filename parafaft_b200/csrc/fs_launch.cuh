@@ -108,8 +108,12 @@ cudaError_t launch_static_pipelined(const PassArgs &a, cudaStream_t st) {
 
 template <typename T, int L, bool COL, bool FWD, int KIND>
 cudaError_t launch_static_var(int var, const PassArgs &a, cudaStream_t st) {
-  if constexpr (!is_pow2(L)) // mixed-radix lengths have the full tile only
+  if constexpr (!is_pow2(L)) { // mixed-radix lengths: full tile, or half for columns
+    if constexpr (COL)
+      if (var == 1)
+        return launch_static_one<T, L, COL, FWD, KIND, 1>(a, st);
     return launch_static_one<T, L, COL, FWD, KIND, 0>(a, st);
+  }
   if constexpr (COL && KIND == KIND_C2C) {
     if (var == kVariantStaged)
       return launch_static_staged<T, L, FWD>(a, st);
