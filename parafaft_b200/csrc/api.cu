@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
@@ -400,6 +401,7 @@ struct GroupStep {
   std::vector<GenArgs> items;
   std::vector<PassArgs> sitems;
   std::vector<long long> tile_start;
+  int2 *d_tile_map = nullptr; // STATIC: (item, tile within the item) per tile
   GenArgs *d_items = nullptr;
   PassArgs *d_sitems = nullptr;
   long long *d_tile_start = nullptr;
@@ -1616,6 +1618,8 @@ void group_free_schedule(G *g) {
         cudaFree(s.d_sitems);
       if (s.d_tile_start)
         cudaFree(s.d_tile_start);
+      if (s.d_tile_map)
+        cudaFree(s.d_tile_map);
     }
     if (g->d_queues)
       cudaFree(g->d_queues);
@@ -1781,15 +1785,23 @@ int group_build(G *g) {
   for (GroupStep &s : g->steps) {
     if (s.type != GroupStep::STATIC)
       continue;
+    const long long ntiles = s.tile_start.back();
+    if (ntiles > INT_MAX)
+      return fail(B200FFT_ERR_RANGE, "b200fft: grouped pass has too many tiles");
+    std::vector<int2> map(static_cast<size_t>(ntiles));
+    for (size_t it = 0; it + 1 < s.tile_start.size(); ++it)
+      for (long long t = s.tile_start[it]; t < s.tile_start[it + 1]; ++t)
+        map[static_cast<size_t>(t)] =
+            make_int2(static_cast<int>(it), static_cast<int>(t - s.tile_start[it]));
     cudaError_t e = cudaMalloc(&s.d_sitems, s.sitems.size() * sizeof(PassArgs));
     if (e == cudaSuccess)
-      e = cudaMalloc(&s.d_tile_start, s.tile_start.size() * sizeof(long long));
+      e = cudaMalloc(&s.d_tile_map, map.size() * sizeof(int2));
     if (e == cudaSuccess)
       e = cudaMemcpy(s.d_sitems, s.sitems.data(), s.sitems.size() * sizeof(PassArgs),
                      cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
-      e = cudaMemcpy(s.d_tile_start, s.tile_start.data(),
-                     s.tile_start.size() * sizeof(long long), cudaMemcpyHostToDevice);
+      e = cudaMemcpy(s.d_tile_map, map.data(), map.size() * sizeof(int2),
+                     cudaMemcpyHostToDevice);
     if (e != cudaSuccess)
       return cuda_fail(e, "group work list upload");
   }
@@ -1865,18 +1877,17 @@ int group_run(G *g) {
                                    s.smem, s.grid, st);
       } else if (s.type == GroupStep::STATIC) {
         what = "grouped specialised pass";
-        const int n = static_cast<int>(s.sitems.size());
         const long long nt = s.tile_start.back();
         if (s.kind == KIND_C2C)
-          e = s.f64 ? launch_static_group_c2c_f64(s.L, s.col, s.fwd, s.d_sitems, s.d_tile_start, n,
+          e = s.f64 ? launch_static_group_c2c_f64(s.L, s.col, s.fwd, s.d_sitems, s.d_tile_map,
                                                   nt, st)
-                    : launch_static_group_c2c_f32(s.L, s.col, s.fwd, s.d_sitems, s.d_tile_start, n,
+                    : launch_static_group_c2c_f32(s.L, s.col, s.fwd, s.d_sitems, s.d_tile_map,
                                                   nt, st);
         else
           e = s.f64 ? launch_static_group_real_f64(s.L, s.kind == KIND_R2C, s.d_sitems,
-                                                   s.d_tile_start, n, nt, st)
+                                                   s.d_tile_map, nt, st)
                     : launch_static_group_real_f32(s.L, s.kind == KIND_R2C, s.d_sitems,
-                                                   s.d_tile_start, n, nt, st);
+                                                   s.d_tile_map, nt, st);
       } else if (s.type == GroupStep::SINGLE) {
         what = "single pass";
         cudaStream_t keep = s.h->stream;

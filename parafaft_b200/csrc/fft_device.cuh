@@ -847,24 +847,17 @@ __global__ void __launch_bounds__(NT, (static_min_blocks<int(sizeof(T) * 2), NT,
 // Grouped specialised pass: the same length and layout for many independent
 // passes (items, e.g. the same stage of many separate grids), each with its
 // own pointers, batch and strides. CTA blockIdx.x runs global tile
-// blockIdx.x; item i covers tiles [tile_start[i], tile_start[i+1]).
+// blockIdx.x: tile_map[blockIdx.x] = (item, tile within the item), built on
+// the host, so a CTA finds its work with one load.
 template <typename T, int L, int NT, int TB, bool COL, bool FWD, int KIND>
 __global__ void __launch_bounds__(NT, (static_min_blocks<int(sizeof(T) * 2), NT, TB, L, COL>()))
     fft_static_group_kernel(const PassArgs *__restrict__ items,
-                            const long long *__restrict__ tile_start, int nitems) {
+                            const int2 *__restrict__ tile_map) {
   using K = KS<T, L, NT, TB, COL, FWD, KIND>;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const long long t = blockIdx.x;
-  int lo = 0, hi = nitems - 1;
-  while (lo < hi) { // last item whose first tile is <= t
-    const int mid = (lo + hi + 1) >> 1;
-    if (tile_start[mid] <= t)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  const PassArgs a = items[lo];
-  K::entry(a, reinterpret_cast<typename K::V *>(smraw), t - tile_start[lo]);
+  const int2 m = tile_map[blockIdx.x];
+  const PassArgs a = items[m.x];
+  K::entry(a, reinterpret_cast<typename K::V *>(smraw), m.y);
 }
 
 template <typename T, int L, int NT, int TB, bool FWD>

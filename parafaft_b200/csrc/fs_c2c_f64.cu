@@ -11,12 +11,12 @@ cudaError_t launch_static_c2c_f64(int L, bool col, bool fwd, int var, const Pass
              : launch_static_switch<double, false, false, KIND_C2C>(L, var, a, st);
 }
 cudaError_t launch_static_group_c2c_f64(int L, bool col, bool fwd, const PassArgs *items,
-                                        const long long *tile_start, int nitems, long long ntiles,
+                                        const int2 *tile_map, long long ntiles,
                                         cudaStream_t st) {
   if (col)
-    return fwd ? launch_static_group_switch<double, true, true, KIND_C2C>(L, items, tile_start, nitems, ntiles, st)
-               : launch_static_group_switch<double, true, false, KIND_C2C>(L, items, tile_start, nitems, ntiles, st);
-  return fwd ? launch_static_group_switch<double, false, true, KIND_C2C>(L, items, tile_start, nitems, ntiles, st)
-             : launch_static_group_switch<double, false, false, KIND_C2C>(L, items, tile_start, nitems, ntiles, st);
+    return fwd ? launch_static_group_switch<double, true, true, KIND_C2C>(L, items, tile_map, ntiles, st)
+               : launch_static_group_switch<double, true, false, KIND_C2C>(L, items, tile_map, ntiles, st);
+  return fwd ? launch_static_group_switch<double, false, true, KIND_C2C>(L, items, tile_map, ntiles, st)
+             : launch_static_group_switch<double, false, false, KIND_C2C>(L, items, tile_map, ntiles, st);
 }
 } // namespace b200fft

@@ -144,8 +144,8 @@ cudaError_t launch_static_var(int var, const PassArgs &a, cudaStream_t st) {
 
 // Grouped specialised pass (full tile): one CTA per tile of every item.
 template <typename T, int L, bool COL, bool FWD, int KIND>
-cudaError_t launch_static_group_one(const PassArgs *items, const long long *tile_start, int nitems,
-                                    long long ntiles, cudaStream_t st) {
+cudaError_t launch_static_group_one(const PassArgs *items, const int2 *tile_map, long long ntiles,
+                                    cudaStream_t st) {
   constexpr CfgS cf = cfg_static(static_cast<int>(sizeof(cvec<T>)), L, COL, 0);
   using K = KS<T, L, cf.NT, cf.TB, COL, FWD, KIND>;
   auto kern = fft_static_group_kernel<T, L, cf.NT, cf.TB, COL, FWD, KIND>;
@@ -166,16 +166,16 @@ cudaError_t launch_static_group_one(const PassArgs *items, const long long *tile
     return cudaSuccess;
   if (ntiles > INT_MAX)
     return cudaErrorInvalidConfiguration;
-  kern<<<static_cast<unsigned>(ntiles), cf.NT, smem, st>>>(items, tile_start, nitems);
+  kern<<<static_cast<unsigned>(ntiles), cf.NT, smem, st>>>(items, tile_map);
   return cudaGetLastError();
 }
 
 #define B2_FG_CASE(LL)                                                         \
-  case LL: return launch_static_group_one<T, LL, COL, FWD, KIND>(items, ts, n, nt, st);
+  case LL: return launch_static_group_one<T, LL, COL, FWD, KIND>(items, tm, nt, st);
 
 template <typename T, bool COL, bool FWD, int KIND>
-cudaError_t launch_static_group_switch(int L, const PassArgs *items, const long long *ts, int n,
-                                       long long nt, cudaStream_t st) {
+cudaError_t launch_static_group_switch(int L, const PassArgs *items, const int2 *tm, long long nt,
+                                       cudaStream_t st) {
   switch (L) {
     B2_FG_CASE(2) B2_FG_CASE(4) B2_FG_CASE(8) B2_FG_CASE(16) B2_FG_CASE(32)
     B2_FG_CASE(64) B2_FG_CASE(128) B2_FG_CASE(256) B2_FG_CASE(512)
@@ -185,7 +185,7 @@ cudaError_t launch_static_group_switch(int L, const PassArgs *items, const long 
     B2_FG_CASE(384) B2_FG_CASE(768)
   case 4096:
     if constexpr (KIND == KIND_C2C)
-      return launch_static_group_one<T, 4096, COL, FWD, KIND>(items, ts, n, nt, st);
+      return launch_static_group_one<T, 4096, COL, FWD, KIND>(items, tm, nt, st);
     else
       return cudaErrorInvalidValue;
   default:

@@ -9,9 +9,9 @@ cudaError_t launch_static_c2r_f64(int L, int var, const PassArgs &a, cudaStream_
   return launch_static_switch<double, false, false, KIND_C2R>(L, var, a, st);
 }
 cudaError_t launch_static_group_real_f64(int L, bool r2c, const PassArgs *items,
-                                         const long long *tile_start, int nitems, long long ntiles,
+                                         const int2 *tile_map, long long ntiles,
                                          cudaStream_t st) {
-  return r2c ? launch_static_group_switch<double, false, true, KIND_R2C>(L, items, tile_start, nitems, ntiles, st)
-             : launch_static_group_switch<double, false, false, KIND_C2R>(L, items, tile_start, nitems, ntiles, st);
+  return r2c ? launch_static_group_switch<double, false, true, KIND_R2C>(L, items, tile_map, ntiles, st)
+             : launch_static_group_switch<double, false, false, KIND_C2R>(L, items, tile_map, ntiles, st);
 }
 } // namespace b200fft

@@ -21,19 +21,19 @@ cudaError_t launch_static_r2c_f64(int L, int var, const PassArgs &a, cudaStream_
 cudaError_t launch_static_c2r_f64(int L, int var, const PassArgs &a, cudaStream_t st);
 
 // Grouped Family S passes (full tile): items are the passes' kernel arguments
-// (device array); item i covers tiles [tile_start[i], tile_start[i+1]) of
-// static_tile_transforms(...) transforms each.
+// (device array); tile_map[t] = (item, tile within the item) for each of the
+// ntiles tiles of static_tile_transforms(...) transforms (device array).
 cudaError_t launch_static_group_c2c_f32(int L, bool col, bool fwd, const PassArgs *items,
-                                        const long long *tile_start, int nitems, long long ntiles,
+                                        const int2 *tile_map, long long ntiles,
                                         cudaStream_t st);
 cudaError_t launch_static_group_c2c_f64(int L, bool col, bool fwd, const PassArgs *items,
-                                        const long long *tile_start, int nitems, long long ntiles,
+                                        const int2 *tile_map, long long ntiles,
                                         cudaStream_t st);
 cudaError_t launch_static_group_real_f32(int L, bool r2c, const PassArgs *items,
-                                         const long long *tile_start, int nitems, long long ntiles,
+                                         const int2 *tile_map, long long ntiles,
                                          cudaStream_t st);
 cudaError_t launch_static_group_real_f64(int L, bool r2c, const PassArgs *items,
-                                         const long long *tile_start, int nitems, long long ntiles,
+                                         const int2 *tile_map, long long ntiles,
                                          cudaStream_t st);
 inline int static_tile_transforms(int esize_complex, int L, bool col) {
   return cfg_static(esize_complex, L, col, 0).TB;
