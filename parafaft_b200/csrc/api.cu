@@ -190,9 +190,11 @@ int default_variant(int csize, int L, bool col, long long stride) {
     // (256 points at a 4 MiB stride 6.4 vs 4.7 TB/s for the wide tile)
     return 0;
   }
-  // rows of 256 (FP32, FP64) and 512 (FP32) points: twice the points per
-  // thread, so the radix-16/32 schedule needs two stages instead of three
-  if ((L == 256 || (L == 512 && csize == 8)))
+  // rows of 256 points (FP32, FP64): twice the points per thread (16), so the
+  // radix-16 schedule needs two stages instead of three. 512-point FP32 rows
+  // keep the full tile (16 points, three CTAs per SM): 0.35 vs 0.36-0.43 ms
+  // for 512^3 C2C rows at 32 points per thread.
+  if (L == 256)
     return 1;
   return 0;
 }

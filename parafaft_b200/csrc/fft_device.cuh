@@ -49,6 +49,24 @@ BF_D uint32_t fdiv(uint32_t n, const FastDiv &f) {
   return f.m == 0 ? n : (__umulhi(n, f.m) >> f.s);
 }
 
+// Slab sl and position w of transform b < a.total (b = sl*batch + w). One
+// slab (the common case, the same for the whole grid) needs no division;
+// otherwise a 32-bit division when the transforms fit, else 64-bit (a 64-bit
+// division is a long software sequence per warp).
+BF_D void slab_of(const PassArgs &a, long long b, long long &sl, long long &w) {
+  if (a.total == a.batch) {
+    sl = 0;
+    w = b;
+  } else if (a.total <= 0xffffffffll) {
+    const unsigned q = static_cast<unsigned>(b) / static_cast<unsigned>(a.batch);
+    sl = q;
+    w = b - static_cast<long long>(q) * a.batch;
+  } else {
+    sl = b / a.batch;
+    w = b - sl * a.batch;
+  }
+}
+
 // ---- small DFTs (natural order in and out) -------------------------------
 template <bool FWD, typename V> BF_D void dft2(V &a, V &b) {
   V t = csub(a, b);
@@ -607,8 +625,8 @@ struct KS {
     c.act = b < a.total;
     long long ioff = 0, ooff = 0;
     if (c.act) {
-      const long long sl = b / a.batch;
-      const long long w = b - sl * a.batch;
+      long long sl, w;
+      slab_of(a, b, sl, w);
       ioff = sl * a.islab + w * a.idist;
       ooff = sl * a.oslab + w * a.odist;
     }
@@ -685,8 +703,8 @@ struct KS {
     c.act = b < a.total;
     long long ioff = 0, ooff = 0;
     if (c.act) {
-      const long long sl = b / a.batch;
-      const long long w = b - sl * a.batch;
+      long long sl, w;
+      slab_of(a, b, sl, w);
       ioff = sl * a.islab + w * a.idist;
       ooff = sl * a.oslab + w * a.odist;
     }
@@ -750,8 +768,8 @@ struct KS {
     const long long b = tile * TB + tb;
     if (b >= a.total)
       return;
-    const long long sl = b / a.batch;
-    const long long w = b - sl * a.batch;
+    long long sl, w;
+    slab_of(a, b, sl, w);
     const V *g = reinterpret_cast<const V *>(a.in) + sl * a.islab + w * a.idist;
     constexpr int ROWS = NT / TB;
 #pragma unroll 8
@@ -789,8 +807,9 @@ struct KS {
       c.act = b < a.total;
       long long ooff = 0;
       if (c.act) {
-        const long long sl = b / a.batch;
-        ooff = sl * a.oslab + (b - sl * a.batch) * a.odist;
+        long long sl, w;
+        slab_of(a, b, sl, w);
+        ooff = sl * a.oslab + w * a.odist;
       }
       c.gout = reinterpret_cast<V *>(a.out) + ooff;
       V v[EMAX];

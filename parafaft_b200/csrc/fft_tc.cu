@@ -228,7 +228,8 @@ __global__ void __launch_bounds__(kRowWarps * 32, row_min_blocks<L>())
 #pragma unroll 1
   for (long long b = static_cast<long long>(blockIdx.x) * kRowWarps + (threadIdx.x >> 5);
        b < a.total; b += nwarp) {
-    const long long sl = b / a.batch, w = b - sl * a.batch;
+    long long sl, w;
+    slab_of(a, b, sl, w);
     const float2 *in = static_cast<const float2 *>(a.in) + sl * a.islab + w * a.idist;
     float2 *out = static_cast<float2 *>(a.out) + sl * a.oslab + w * a.odist;
     const long long is = a.istride, os = a.ostride;
@@ -376,7 +377,8 @@ __global__ void __launch_bounds__(ColCfg<L>::NT, ColCfg<L>::NT == 512 ? 1 : 2)
       const long long b = tile * 16 + tid;
       long long io = -1, oo = -1;
       if (b < a.total) {
-        const long long sl = b / a.batch, w = b - sl * a.batch;
+        long long sl, w;
+        slab_of(a, b, sl, w);
         io = sl * a.islab + w * a.idist;
         oo = sl * a.oslab + w * a.odist;
       }

@@ -233,7 +233,8 @@ __global__ void __launch_bounds__(kTc5Threads, 8) fft_tc5_row256_kernel(PassArgs
     const bool act = b < a.total;
     long long io = 0, oo = 0;
     if (act) {
-      const long long sl = b / a.batch, w = b - sl * a.batch;
+      long long sl, w;
+      slab_of(a, b, sl, w);
       io = sl * a.islab + w * a.idist;
       oo = sl * a.oslab + w * a.odist;
     }

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(NT, 1)
 
   // thread 0: the copies of tile `tile` into buffer s, completing on full[s]
   auto issue = [&](long long tile, int s) {
-    const long long sl = tile / tiles_per_slab;
+    const long long sl = ntiles == tiles_per_slab ? 0 : tile / tiles_per_slab;
     const int x = static_cast<int>((tile - sl * tiles_per_slab) * TB * 2); // floats
     const uint32_t mb = su32(&full[s]);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(NT, 1)
       return;
     }
     c.sm = ring + static_cast<size_t>(s) * L * TB;
-    const long long sl = tile / tiles_per_slab;
+    const long long sl = ntiles == tiles_per_slab ? 0 : tile / tiles_per_slab;
     const long long w = (tile - sl * tiles_per_slab) * TB + c.tb;
     c.act = w < a.batch;
     c.gout = reinterpret_cast<V *>(a.out) + (c.act ? sl * a.oslab + w * a.odist : 0);
