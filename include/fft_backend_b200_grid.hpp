@@ -30,9 +30,11 @@
  *  - R2C buffer (get_real_buffer): [N0]...[N_{D-2}][2*(N_{D-1}/2+1)] reals,
  *    ParaFaFT's padded in-place layout (parafaft_r2c.hpp:804-847); after the
  *    forward transform it holds [N0]...[N_{D-2}][N_{D-1}/2+1] complex.
- * Both buffers are allocated by setup_distributed(). As with cuFFTMp,
- * get_distributed_info() describes the C2C grid (required_size in complex
- * elements).
+ * Each side is set up on first use: get_buffer()/forward()/backward()
+ * allocate and plan the C2C grid, get_real_buffer()/forward_r2c()/
+ * backward_c2r() the R2C one, so an object holds only the grid its
+ * orchestrator transforms. As with cuFFTMp, get_distributed_info() describes
+ * the C2C grid (required_size in complex elements).
  *
  * Results are those of B200Backend<T> through the per-stage path (the same
  * kernels on the same passes); transforms are unnormalised.
@@ -94,7 +96,8 @@ public:
   B200GridBackend &operator=(const B200GridBackend &) = delete;
   B200GridBackend(B200GridBackend &&o) noexcept
       : plan_flag_(o.plan_flag_), comm_(o.comm_), shape_(o.shape_), info_(o.info_),
-        cbuf_(std::move(o.cbuf_)), rbuf_(std::move(o.rbuf_)), copy_h_(o.copy_h_) {
+        cbuf_(std::move(o.cbuf_)), rbuf_(std::move(o.rbuf_)), copy_h_(o.copy_h_),
+        ready_(o.ready_) {
     for (int t = 0; t < kTransforms; ++t) {
       h_[t] = o.h_[t];
       g_[t] = o.g_[t];
@@ -102,6 +105,7 @@ public:
       o.g_[t] = nullptr;
     }
     o.copy_h_ = nullptr;
+    o.ready_ = false;
   }
 
   // ---- distributed part of the concept (fft_backend.hpp:153-190) ----------
@@ -113,6 +117,7 @@ public:
                                std::to_string(size) + " ranks");
     comm_ = comm;
     release();
+    ready_ = false;
     long long n = 1;
     for (int i = 0; i < D; ++i) {
       if (global_shape[i] < 1)
@@ -123,26 +128,37 @@ public:
       info_.global_start[i] = info_.output_start[i] = 0;
     }
     info_.required_size = static_cast<std::size_t>(n);
-    const long long rows = n / shape_[D - 1];
-    const long long nh = shape_[D - 1] / 2 + 1;
-    cbuf_.resize(static_cast<std::size_t>(n));
-    rbuf_.resize(static_cast<std::size_t>(rows * 2 * nh));
     open(copy_h_, 1);
-    build_c2c(kC2CForward, B200FFT_FORWARD);
-    build_c2c(kC2CBackward, B200FFT_BACKWARD);
-    build_real(kR2C);
-    build_real(kC2R);
+    ready_ = true;
   }
 
   DistributedInfo get_distributed_info() const { return info_; }
 
-  Complex *get_buffer() { return cbuf_.data(); }
-  FloatType *get_real_buffer() { return rbuf_.data(); }
+  Complex *get_buffer() {
+    ensure_c2c();
+    return cbuf_.data();
+  }
+  FloatType *get_real_buffer() {
+    ensure_real();
+    return rbuf_.data();
+  }
 
-  void forward() { run(kC2CForward); }
-  void backward() { run(kC2CBackward); }
-  void forward_r2c() { run(kR2C); }
-  void backward_c2r() { run(kC2R); }
+  void forward() {
+    ensure_c2c();
+    run(kC2CForward);
+  }
+  void backward() {
+    ensure_c2c();
+    run(kC2CBackward);
+  }
+  void forward_r2c() {
+    ensure_real();
+    run(kR2C);
+  }
+  void backward_c2r() {
+    ensure_real();
+    run(kC2R);
+  }
 
   // ---- the rest of the concept ----------------------------------------------
   void memcpy(void *dest, const void *src, std::size_t bytes) const {
@@ -178,6 +194,26 @@ public:
 
 private:
   enum { kC2CForward = 0, kC2CBackward = 1, kR2C = 2, kC2R = 3, kTransforms = 4 };
+
+  void ensure_c2c() {
+    if (!ready_)
+      throw std::runtime_error("B200GridBackend: setup_distributed was not called");
+    if (g_[kC2CForward] != nullptr)
+      return;
+    cbuf_.resize(info_.required_size);
+    build_c2c(kC2CForward, B200FFT_FORWARD);
+    build_c2c(kC2CBackward, B200FFT_BACKWARD);
+  }
+  void ensure_real() {
+    if (!ready_)
+      throw std::runtime_error("B200GridBackend: setup_distributed was not called");
+    if (g_[kR2C] != nullptr)
+      return;
+    const long long rows = static_cast<long long>(info_.required_size) / shape_[D - 1];
+    rbuf_.resize(static_cast<std::size_t>(rows * 2 * (shape_[D - 1] / 2 + 1)));
+    build_real(kR2C);
+    build_real(kC2R);
+  }
 
   void open(b200fft_handle &h, int stages) {
     const int prec = std::is_same<FloatType, double>::value ? B200FFT_F64 : B200FFT_F32;
@@ -289,8 +325,6 @@ private:
   }
 
   void run(int t) {
-    if (g_[t] == nullptr)
-      throw std::runtime_error("B200GridBackend: setup_distributed was not called");
     b200_detail::check(b200fft_group_replay(g_[t]), "replay");
     b200_detail::check(b200fft_group_sync(g_[t]), "wait");
   }
@@ -318,6 +352,7 @@ private:
   b200fft_handle h_[kTransforms] = {nullptr, nullptr, nullptr, nullptr};
   b200fft_group g_[kTransforms] = {nullptr, nullptr, nullptr, nullptr};
   b200fft_handle copy_h_ = nullptr;
+  bool ready_ = false; // setup_distributed has run
 };
 
 } // namespace parafaft
