@@ -219,8 +219,11 @@ int b200fft_group_stats(b200fft_group g, b200fft_stats *out);
  * lives in a fixed 128 KiB array inside the library, so `length` must be a
  * power of two from 2 to 4096 (anything else returns B200FFT_ERR_UNSUPPORTED).
  * The first call on a device resolves that array's address; make it before any
- * stream capture. All calls on a device share the array: calls that may run
- * concurrently on the GPU race, so order them on one stream. */
+ * stream capture. The address is kept for the life of the process, so calls
+ * after cudaDeviceReset on that device are not supported. All calls on a
+ * device share the array: calls that may run concurrently on the GPU race, so
+ * order them on one stream. Columns run on the default tile of the length
+ * (no per-stride tile choice, unlike a handle's plan). */
 int b200fft_c2c_noalloc(int precision, int direction, int length, size_t batch,
                         ptrdiff_t stride, ptrdiff_t dist, const void *in, void *out,
                         void *cuda_stream);

@@ -97,7 +97,7 @@ public:
   B200GridBackend(B200GridBackend &&o) noexcept
       : plan_flag_(o.plan_flag_), comm_(o.comm_), shape_(o.shape_), info_(o.info_),
         cbuf_(std::move(o.cbuf_)), rbuf_(std::move(o.rbuf_)), copy_h_(o.copy_h_),
-        ready_(o.ready_) {
+        ready_(o.ready_), c2c_built_(o.c2c_built_), real_built_(o.real_built_) {
     for (int t = 0; t < kTransforms; ++t) {
       h_[t] = o.h_[t];
       g_[t] = o.g_[t];
@@ -106,6 +106,7 @@ public:
     }
     o.copy_h_ = nullptr;
     o.ready_ = false;
+    o.c2c_built_ = o.real_built_ = false;
   }
 
   // ---- distributed part of the concept (fft_backend.hpp:153-190) ----------
@@ -195,24 +196,42 @@ public:
 private:
   enum { kC2CForward = 0, kC2CBackward = 1, kR2C = 2, kC2R = 3, kTransforms = 4 };
 
+  // A side (C2C, or R2C with C2R) counts as built only once both of its
+  // transforms are recorded and captured; if either build throws, the
+  // handles and groups of that side are released so the next call starts
+  // again from nothing.
   void ensure_c2c() {
     if (!ready_)
       throw std::runtime_error("B200GridBackend: setup_distributed was not called");
-    if (g_[kC2CForward] != nullptr)
+    if (c2c_built_)
       return;
-    cbuf_.resize(info_.required_size);
-    build_c2c(kC2CForward, B200FFT_FORWARD);
-    build_c2c(kC2CBackward, B200FFT_BACKWARD);
+    try {
+      cbuf_.resize(info_.required_size);
+      build_c2c(kC2CForward, B200FFT_FORWARD);
+      build_c2c(kC2CBackward, B200FFT_BACKWARD);
+    } catch (...) {
+      release_transform(kC2CForward);
+      release_transform(kC2CBackward);
+      throw;
+    }
+    c2c_built_ = true;
   }
   void ensure_real() {
     if (!ready_)
       throw std::runtime_error("B200GridBackend: setup_distributed was not called");
-    if (g_[kR2C] != nullptr)
+    if (real_built_)
       return;
-    const long long rows = static_cast<long long>(info_.required_size) / shape_[D - 1];
-    rbuf_.resize(static_cast<std::size_t>(rows * 2 * (shape_[D - 1] / 2 + 1)));
-    build_real(kR2C);
-    build_real(kC2R);
+    try {
+      const long long rows = static_cast<long long>(info_.required_size) / shape_[D - 1];
+      rbuf_.resize(static_cast<std::size_t>(rows * 2 * (shape_[D - 1] / 2 + 1)));
+      build_real(kR2C);
+      build_real(kC2R);
+    } catch (...) {
+      release_transform(kR2C);
+      release_transform(kC2R);
+      throw;
+    }
+    real_built_ = true;
   }
 
   void open(b200fft_handle &h, int stages) {
@@ -329,15 +348,18 @@ private:
     b200_detail::check(b200fft_group_sync(g_[t]), "wait");
   }
 
+  void release_transform(int t) {
+    if (g_[t])
+      b200fft_group_destroy(g_[t]);
+    if (h_[t])
+      b200fft_destroy(h_[t]);
+    g_[t] = nullptr;
+    h_[t] = nullptr;
+  }
   void release() {
-    for (int t = 0; t < kTransforms; ++t) {
-      if (g_[t])
-        b200fft_group_destroy(g_[t]);
-      if (h_[t])
-        b200fft_destroy(h_[t]);
-      g_[t] = nullptr;
-      h_[t] = nullptr;
-    }
+    for (int t = 0; t < kTransforms; ++t)
+      release_transform(t);
+    c2c_built_ = real_built_ = false;
     if (copy_h_)
       b200fft_destroy(copy_h_);
     copy_h_ = nullptr;
@@ -352,7 +374,9 @@ private:
   b200fft_handle h_[kTransforms] = {nullptr, nullptr, nullptr, nullptr};
   b200fft_group g_[kTransforms] = {nullptr, nullptr, nullptr, nullptr};
   b200fft_handle copy_h_ = nullptr;
-  bool ready_ = false; // setup_distributed has run
+  bool ready_ = false;      // setup_distributed has run
+  bool c2c_built_ = false;  // both C2C transforms recorded and captured
+  bool real_built_ = false; // R2C and C2R recorded and captured
 };
 
 } // namespace parafaft

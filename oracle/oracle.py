@@ -139,6 +139,30 @@ def r2c_nd(x: np.ndarray, impl: str = "c") -> np.ndarray:
     return out
 
 
+def c2c_planes(slab, n0: int, k0s, block: int = 16) -> np.ndarray:
+    """Output planes X[k0, :, :] of the unnormalised forward 3-D C2C of a grid
+    too large for a full FP64 copy, in FP64 (scipy.fft / pocketfft):
+
+        X[k0, :, :] = sum_n0 exp(-2 pi i k0 n0 / N0) * fft2(x[n0, :, :]).
+
+    `slab(a, b)` returns x[a:b] (any complex dtype; promoted to complex128).
+    The phase is reduced exactly in integers ((k0 * n0) mod N0) before the
+    FP64 exponential. Slabs are taken `block` at a time and the planes are
+    accumulated as one (K x block) x (block x plane) product."""
+    import scipy.fft as sf
+    k0s = np.asarray(list(k0s), dtype=np.int64)
+    acc = None
+    for a in range(0, n0, block):
+        b = min(a + block, n0)
+        xs = np.asarray(slab(a, b), dtype=np.complex128)
+        F = sf.fft2(xs, axes=(-2, -1), workers=os.cpu_count())
+        m = (k0s[:, None] * np.arange(a, b, dtype=np.int64)[None, :]) % n0
+        w = np.exp(-2j * np.pi * (m.astype(np.float64) / n0))
+        part = (w @ F.reshape(b - a, -1)).reshape((len(k0s),) + F.shape[1:])
+        acc = part if acc is None else acc + part
+    return acc
+
+
 def c2r_nd(X: np.ndarray, n_last: int, impl: str = "c") -> np.ndarray:
     """n-D C2R (unnormalised); Im of DC/Nyquist of the last axis ignored."""
     X = np.ascontiguousarray(X, dtype=np.complex128)

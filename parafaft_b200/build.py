@@ -4,10 +4,13 @@
   (``include/b200fft.h``), compiled for sm_100a only.
 * ``parafaft_b200/lib/libparafaft_b200_drivers.so`` — ParaFaFT's own
   ``ParaFaFT_C2C``/``ParaFaFT_R2C`` orchestrators instantiated with
-  ``B200Backend<T>`` (and, for comparison, the reference ``CuFFTBackend<T>``),
-  behind a small C ABI used by the tests and the benchmark. It needs the
-  ParaFaFT headers at compile time, so it is only (re)built where they exist;
-  elsewhere the prebuilt library is used as is.
+  ``B200Backend<T>`` and ``B200GridBackend<D, T>``, behind a small C ABI used
+  by the tests and the benchmark. It does not link cuFFT.
+* ``parafaft_b200/lib/libparafaft_cufft_drivers.so`` — the same orchestrators
+  on the reference ``CuFFTBackend<T>`` as well (the comparison on the same
+  GPU); the only library that links cuFFT.
+Both need the ParaFaFT headers at compile time, so they are only (re)built
+where those exist; elsewhere the prebuilt libraries are used as they are.
 
 Run as ``python -m parafaft_b200.build [--force]``.
 """
@@ -29,6 +32,7 @@ INCLUDE = ROOT / "include"
 
 ENGINE_SO = LIB / "libb200fft.so"
 DRIVERS_SO = LIB / "libparafaft_b200_drivers.so"
+CUFFT_DRIVERS_SO = LIB / "libparafaft_cufft_drivers.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC"] + ARCH
@@ -44,9 +48,10 @@ def _nvcc() -> str:
 
 
 def reference_root() -> Path | None:
-    """ParaFaFT source tree, if present on this machine."""
+    """ParaFaFT source tree, if present on this machine: $PARAFAFT_ROOT, else a
+    ``reference`` checkout beside this repository."""
     env = os.environ.get("PARAFAFT_ROOT")
-    for c in ([Path(env)] if env else []) + [Path("/root/reference")]:
+    for c in ([Path(env)] if env else []) + [ROOT.parent / "reference"]:
         if (c / "parafaft_r2c.hpp").exists():
             return c
     return None
@@ -94,10 +99,18 @@ def build_drivers(force: bool = False) -> Path | None:
     deps = [src, INCLUDE / "fft_backend_b200.hpp", INCLUDE / "fft_backend_b200_grid.hpp",
             INCLUDE / "b200fft.h",
             INTEG / "mpi_shim" / "mpi.h", ENGINE_SO]
+    common = [_nvcc(), *NVCC_FLAGS, "-I", str(INCLUDE), "-I", str(INTEG / "mpi_shim"),
+              "-I", str(ref), "-shared", str(src)]
+    jobs = []
     if force or _newer(DRIVERS_SO, deps):
-        _run([_nvcc(), *NVCC_FLAGS, "-I", str(INCLUDE), "-I", str(INTEG / "mpi_shim"),
-              "-I", str(ref), "-shared", str(src), "-o", str(DRIVERS_SO),
-              "-L", str(LIB), "-lb200fft", "-lcufft", "-Xlinker", "-rpath,$ORIGIN"])
+        jobs.append(common + ["-o", str(DRIVERS_SO), "-L", str(LIB), "-lb200fft",
+                              "-Xlinker", "-rpath,$ORIGIN"])
+    if force or _newer(CUFFT_DRIVERS_SO, deps):
+        jobs.append(common + ["-DPFB_WITH_CUFFT", "-o", str(CUFFT_DRIVERS_SO), "-L", str(LIB),
+                              "-lb200fft", "-lcufft", "-Xlinker", "-rpath,$ORIGIN"])
+    if jobs:
+        with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+            list(ex.map(_run, jobs))
     return DRIVERS_SO
 
 

@@ -21,6 +21,11 @@
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (once per device, with that device current); make
 //    that first call before any stream capture begins;
+//  * the address is kept for the life of the process: calls after
+//    cudaDeviceReset on that device are not supported (the module, and with
+//    it the array, may move);
+//  * the transform runs the specialised kernel's default tile (variant 0)
+//    whatever the stride; a handle's plan may pick a wider column tile;
 //  * every call on a device shares the one array and leaves its table there:
 //    two calls that can run at the same time on the GPU (different streams
 //    without ordering between them) race on it. Order them on one stream or

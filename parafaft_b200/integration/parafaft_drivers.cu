@@ -15,6 +15,12 @@
 namespace parafaft {
 template <typename FloatTypeT = double> class FFTWBackend;
 }
+// The product build (libparafaft_b200_drivers.so) leaves the reference's
+// cuFFT backend out, so it does not link cuFFT; the comparator build
+// (libparafaft_cufft_drivers.so, compiled with PFB_WITH_CUFFT) adds it.
+#ifndef PFB_WITH_CUFFT
+#define PARAFAFT_BACKEND_CUFFT_HPP 1
+#endif
 
 #include <mpi.h>
 
@@ -222,9 +228,14 @@ Obj *make(int D, int prec, int backend, const int *shape, int plan_flag) {
   if (backend == 0)
     return prec == B200FFT_F64 ? make_d<O, parafaft::B200Backend<double>>(D, shape, flag)
                                : make_d<O, parafaft::B200Backend<float>>(D, shape, flag);
+#ifdef PFB_WITH_CUFFT
   if (backend == 1)
     return prec == B200FFT_F64 ? make_d<O, parafaft::CuFFTBackend<double>>(D, shape, flag)
                                : make_d<O, parafaft::CuFFTBackend<float>>(D, shape, flag);
+#else
+  if (backend == 1)
+    throw std::runtime_error("CuFFTBackend objects live in libparafaft_cufft_drivers.so");
+#endif
   throw std::runtime_error("backend must be 0 (B200Backend) or 1 (CuFFTBackend)");
 }
 

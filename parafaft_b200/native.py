@@ -2,7 +2,9 @@
 
 * ``libb200fft.so`` — the transform engine's C ABI (include/b200fft.h).
 * ``libparafaft_b200_drivers.so`` — ParaFaFT_C2C / ParaFaFT_R2C objects (the
-  reference orchestrators, compiled against B200Backend or CuFFTBackend).
+  reference orchestrators, compiled against B200Backend / B200GridBackend).
+* ``libparafaft_cufft_drivers.so`` — the same, also on the reference
+  CuFFTBackend (the comparison on the same GPU; loaded only for it).
 
 Nothing here computes on the CPU: if a library is missing the loaders raise,
 and the engine itself refuses to create a handle without a CUDA device (except
@@ -17,6 +19,7 @@ from pathlib import Path
 LIB_DIR = Path(__file__).resolve().parent / "lib"
 ENGINE_PATH = LIB_DIR / "libb200fft.so"
 DRIVERS_PATH = LIB_DIR / "libparafaft_b200_drivers.so"
+CUFFT_DRIVERS_PATH = LIB_DIR / "libparafaft_cufft_drivers.so"
 
 F32, F64 = 0, 1
 FORWARD, BACKWARD = 0, 1
@@ -75,7 +78,7 @@ class LaunchRecord(C.Structure):
 
 
 _engine = None
-_drivers = None
+_drivers = {}
 
 
 def engine() -> C.CDLL:
@@ -135,14 +138,16 @@ def engine() -> C.CDLL:
     return _engine
 
 
-def drivers() -> C.CDLL:
-    """Load the ParaFaFT driver library (raises if it has not been built)."""
-    global _drivers
-    if _drivers is None:
+def drivers(cufft: bool = False) -> C.CDLL:
+    """Load the ParaFaFT driver library (raises if it has not been built):
+    the B200 one, or with `cufft` the comparator build that also holds
+    CuFFTBackend objects."""
+    path = CUFFT_DRIVERS_PATH if cufft else DRIVERS_PATH
+    if path not in _drivers:
         engine()  # resolve libb200fft first
-        if not DRIVERS_PATH.exists():
-            raise ImportError(f"{DRIVERS_PATH} is missing: build it where the ParaFaFT headers exist")
-        lib = C.CDLL(str(DRIVERS_PATH))
+        if not path.exists():
+            raise ImportError(f"{path} is missing: build it where the ParaFaFT headers exist")
+        lib = C.CDLL(str(path))
         vp, i = C.c_void_p, C.c_int
         ip = C.POINTER(C.c_int)
         for name, res, args in (
@@ -161,8 +166,8 @@ def drivers() -> C.CDLL:
             fn = getattr(lib, name)
             fn.restype = res
             fn.argtypes = args
-        _drivers = lib
-    return _drivers
+        _drivers[path] = lib
+    return _drivers[path]
 
 
 def check(rc: int) -> None:
@@ -378,7 +383,7 @@ class ParaFaFT:
 
     def __init__(self, kind: str, shape, precision: int = F32, backend: str = "b200",
                  plan_flag: int = PLAN_ESTIMATE):
-        self._lib = drivers()
+        self._lib = drivers(cufft=backend == "cufft")
         self.kind = kind
         self.shape = tuple(int(s) for s in shape)
         self.D = len(self.shape)

@@ -115,3 +115,13 @@ def test_reference_orchestrator_c2c_bug_on_non_cubic_shapes():
     assert f.shapes()[2] != [8, 6, 4, 5]
     g = O.RefParaFaFT("r2c", (8, 6, 10))
     assert g.shapes()[2] == [8, 6, 6]
+
+
+def test_plane_oracle_matches_full_transform():
+    """c2c_planes (the FP64 check of grids too large for a full FP64 copy)
+    against the C oracle's full 3-D transform of the same complex64 input."""
+    x = O.normal_complex((24, 16, 20), 5).astype(np.complex64)
+    ks = [0, 1, 7, 12, 23]
+    planes = O.c2c_planes(lambda a, b: x[a:b], 24, ks, block=5)
+    full = O.c2c_nd(x.astype(np.complex128))
+    assert O.rel_l2(planes, full[ks]) < 1e-14
