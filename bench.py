@@ -216,17 +216,21 @@ def run_kernels_only(args):
     from parafaft_b200 import native as nv
     torch.cuda.set_device(0)
     if args.config in C2C_CONFIGS:
-        shape, prec_s, kind, _, seed = C2C_CONFIGS[args.config]
+        shape, prec_s, _, seed = C2C_CONFIGS[args.config]
         prec = nv.F64 if prec_s == "f64" else nv.F32
-        f = nv.ParaFaFT(kind, shape, prec)
+        # the 4-D grid runs through the grid-owning backend (as in the bench)
+        grid = args.config == "c2c4d"
+        f = nv.ParaFaFT("c2c", shape, prec, backend="b200grid" if grid else "b200")
         gen = torch.Generator(device="cuda").manual_seed(seed)
-        data = torch.randn(f.required_size, generator=gen, device="cuda",
-                           dtype=torch.complex128 if prec == nv.F64 else torch.complex64)
+        ctype = torch.complex128 if prec == nv.F64 else torch.complex64
+        data = f.buffer() if grid else torch.empty(f.required_size, dtype=ctype, device="cuda")
+        data.copy_(torch.randn(data.numel(), generator=gen, device="cuda", dtype=ctype))
+        arg = None if grid else data
         for _ in range(args.warmup + args.steps):
-            f.forward(data)
-            f.backward(data)
+            f.forward(arg)
+            f.backward(arg)
         torch.cuda.synchronize()
-        print("kernels-only done", f.handle().stats()["kernel_launches"])
+        print("kernels-only done", "grid backend" if grid else f.handle().stats()["kernel_launches"])
         f.close()
         return 0
     if args.config == "uneven256":
@@ -301,131 +305,199 @@ def run_single_pass(args):
 
 
 C2C_CONFIGS = {
-    # name: (shape, precision, orchestrator, input distribution, seed)
-    "c2c64": ((64, 64, 64), "f64", "c2c", "uniform", 11),
-    "c2c1024": ((1024, 1024, 1024), "f32", "c2c", "normal", 12),
-    "c2c4d": ((128, 128, 64, 64), "f64", "c2c_onerank", "uniform", 13),
+    # name: (shape, precision, input distribution, seed)
+    "c2c64": ((64, 64, 64), "f64", "uniform", 11),
+    "c2c1024": ((1024, 1024, 1024), "f32", "normal", 12),
+    "c2c4d": ((128, 128, 64, 64), "f64", "uniform", 13),
 }
+# output planes X[k0, :, :] checked against the FP64 plane oracle at 1024^3
+C2_PLANES = (0, 1, 333, 512, 1023)
 
 
-def run_c2c_config(args):
-    """C2C forward+backward through ParaFaFT on B200Backend:
-      c2c64    64^3 complex128, ParaFaFT_C2C<3, B200Backend<double>>;
-      c2c1024  1024^3 complex64, ParaFaFT_C2C<3, B200Backend<float>>;
-      c2c4d    128x128x64x64 complex128 through the one-rank orchestrator (the
-               reference ParaFaFT_C2C mis-sizes non-hypercubic grids).
-    Accuracy: forward rel-L2 against an FP64 reference (the C oracle for 64^3,
-    scipy.fft FP64 for the 4D grid, the B200 FP64 path for 1024^3 whose
-    complex128 copy would not fit a host comparison) and the round trip."""
+def _timed_steps(fn, steps, warmup, stream=None, clocks=None):
+    """ms per call of fn() over `steps` calls after `warmup` untimed ones
+    (CUDA events on `stream`, default: torch's current stream)."""
     import torch
-    from parafaft_b200 import native as nv
-    from oracle import oracle as O
-    torch.cuda.set_device(0)
-    shape, prec_s, kind, dist, seed = C2C_CONFIGS[args.config]
-    prec = nv.F64 if prec_s == "f64" else nv.F32
-    ctype = torch.complex128 if prec == nv.F64 else torch.complex64
-    n = int(np.prod(shape))
-    gen = torch.Generator(device="cuda").manual_seed(seed)
-    if dist == "uniform":
-        re = torch.rand(n, generator=gen, device="cuda", dtype=torch.float64) * 2 - 1
-        im = torch.rand(n, generator=gen, device="cuda", dtype=torch.float64) * 2 - 1
-    else:
-        re = torch.randn(n, generator=gen, device="cuda", dtype=torch.float64)
-        im = torch.randn(n, generator=gen, device="cuda", dtype=torch.float64)
-    x64 = torch.complex(re, im)
-    del re, im
-    f = nv.ParaFaFT(kind, shape, prec)
-    assert f.required_size >= n
-    data = torch.zeros(f.required_size, dtype=ctype, device="cuda")
-    data[:n] = x64.to(ctype)
-    # ---- accuracy
-    f.forward(data)
-    y = data[:n].clone()
-    if args.config == "c2c64":
-        ref = torch.from_numpy(O.c2c_nd(x64.cpu().numpy().reshape(shape)).reshape(-1)).cuda()
-        ref_src = "C oracle FP64"
-    elif args.config == "c2c4d":
-        ref = torch.from_numpy(O.c2c_nd(x64.cpu().numpy().reshape(shape), -1, "scipy").reshape(-1)).cuda()
-        ref_src = "scipy.fft FP64"
-    else:
-        g64 = nv.ParaFaFT(kind, shape, nv.F64)
-        d64 = torch.zeros(g64.required_size, dtype=torch.complex128, device="cuda")
-        d64[:n] = x64
-        g64.forward(d64)
-        ref = d64[:n]
-        ref_src = "B200 FP64 path"
-    rel_fwd = float(torch.linalg.vector_norm(y.to(torch.complex128) - ref) /
-                    torch.linalg.vector_norm(ref))
-    del ref
-    if args.config == "c2c1024":
-        del d64, g64
-    f.backward(data)
-    rel_rt = float(torch.linalg.vector_norm(data[:n].to(torch.complex128) / n - x64) /
-                   torch.linalg.vector_norm(x64))
-    del y
-    # ---- timing
-    data[:n] = x64.to(ctype)
-    del x64
-    h = f.handle()
-    stream = torch.cuda.Stream()
-    h.set_stream(stream.cuda_stream)
-    for _ in range(args.warmup):
-        f.forward(data)
-        f.backward(data)
+    for _ in range(warmup):
+        fn()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    h.reset_stats()
+    if clocks:
+        clocks.mark("t0")
     e0.record(stream)
-    for _ in range(args.steps):
-        f.forward(data)
-        f.backward(data)
+    for _ in range(steps):
+        fn()
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    st = h.stats()
-    h.set_profiling(True)
-    h.reset_stats()
-    for _ in range(max(2, args.steps // 4)):
-        f.forward(data)
-        f.backward(data)
-    log = h.log()
-    h.set_profiling(False)
-    per = {}
-    for r in log:
-        if r["kind"] == 3:
-            continue
-        key = f"stage{r['stage']}_" + ("fwd" if r["direction"] == 0 else "bwd")
-        per.setdefault(key, []).append((r["ms"], r["bytes"]))
-    kernels = {k: {"ms": round(float(np.mean([m for m, _ in v])), 4),
-                   "GBps": round(v[0][1] / np.mean([m for m, _ in v]) / 1e6, 1)} for k, v in per.items()}
+    if clocks:
+        clocks.mark("t1")
+    return e0.elapsed_time(e1) / steps
+
+
+def _rel_dev(y, ref, chunk=1 << 26):
+    """rel-L2 of two device tensors of the same length, in FP64, by chunks."""
+    import torch
+    num = den = 0.0
+    for a in range(0, ref.numel(), chunk):
+        r = ref[a:a + chunk].to(torch.complex128 if ref.is_complex() else torch.float64)
+        d = y[a:a + chunk].to(r.dtype) - r
+        num += float(torch.linalg.vector_norm(d)) ** 2
+        den += float(torch.linalg.vector_norm(r)) ** 2
+    return (num / den) ** 0.5
+
+
+def _env_split_tc(on: bool):
+    """Context for B200FFT_SPLIT_TC (read when a backend handle is created)."""
+    import contextlib
+
+    @contextlib.contextmanager
+    def cm():
+        old = os.environ.get("B200FFT_SPLIT_TC")
+        if on:
+            os.environ["B200FFT_SPLIT_TC"] = "1"
+        else:
+            os.environ.pop("B200FFT_SPLIT_TC", None)
+        try:
+            yield
+        finally:
+            if old is None:
+                os.environ.pop("B200FFT_SPLIT_TC", None)
+            else:
+                os.environ["B200FFT_SPLIT_TC"] = old
+    return cm()
+
+
+def measure_c2c(name, steps, warmup, gpu_index=0):
+    """C2C forward+backward of one of C2C_CONFIGS through the reference
+    ParaFaFT_C2C orchestrator:
+      c2c64    64^3 complex128: ParaFaFT_C2C<3, B200Backend<double>> (per-stage
+               backend) and ParaFaFT_C2C<3, B200GridBackend<3, double>>;
+               forward checked against the C oracle (FP64, full grid).
+      c2c1024  1024^3 complex64: ParaFaFT_C2C<3, B200Backend<float>>, plain and
+               split-TC; forward checked on the output planes C2_PLANES against
+               the FP64 plane oracle (scipy.fft on the same complex64 input).
+      c2c4d    128x128x64x64 complex128: ParaFaFT_C2C<4, B200GridBackend<4,
+               double>> (the reference orchestrator's own path for a grid-owning
+               backend; its per-stage path mis-sizes non-hypercubic grids,
+               parafaft_c2c.hpp:826-831); forward checked against scipy.fft FP64
+               on the full grid.
+    Returns a dict: ms, alg_bytes, hbm_frac, rel-L2 forward and round trip,
+    launches per step, clocks."""
+    import torch
+    from parafaft_b200 import native as nv
+    from oracle import oracle as O
+    torch.cuda.set_device(gpu_index)
+    shape, prec_s, dist, seed = C2C_CONFIGS[name]
+    prec = nv.F64 if prec_s == "f64" else nv.F32
+    ctype = torch.complex128 if prec == nv.F64 else torch.complex64
+    n = int(np.prod(shape))
     esz = 16 if prec == nv.F64 else 8
-    alg = 2 * len(shape) * 2 * n * esz
+    alg = 2 * len(shape) * 2 * n * esz  # one read + one write per pass, fwd+bwd
     peak, peak_kind = _peaks()
-    line = {
-        "metric": f"{args.config} C2C fwd+bwd ms", "value": round(ms, 4), "unit": "ms",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
-        "dtype": prec_s, "data": f"synthetic {dist} complex, seed {seed}",
-        "config": {"workload": f"{kind} {'x'.join(map(str, shape))} {prec_s}", "orchestrator": kind},
-        "form": args.form,
-        "rel_l2_fwd": rel_fwd, "rel_l2_reference": ref_src, "rel_l2_roundtrip": rel_rt,
-        "alg_bytes": alg, "hbm_frac": round(alg / (ms * 1e-3) / 1e9 / peak, 4),
-        "peak_source": peak_kind, "kernels": kernels,
-        "gpu_launches_per_step": st["kernel_launches"] / args.steps,
-        "copies_issued_per_step": st["copies_issued"] / args.steps,
-    }
-    f.close()
-    if args.form == "plain":
-        # fresh input (the timing loop above left unnormalised round trips in data)
+    out = {"workload": f"{'x'.join(map(str, shape))} C2C {'complex128' if prec == nv.F64 else 'complex64'}",
+           "input": f"re, im i.i.d. {'U[-1,1)' if dist == 'uniform' else 'N(0,1)'}, seed {seed}",
+           "alg_bytes": alg, "peak_gbs": peak, "peak_source": peak_kind}
+
+    # ---- input (the oracle sees exactly the values the GPU transforms)
+    if name == "c2c1024":
+        gen = torch.Generator(device="cuda").manual_seed(seed)
+        x0 = torch.complex(torch.randn(n, generator=gen, device="cuda"),
+                           torch.randn(n, generator=gen, device="cuda"))
+        x_host = None
+    else:
+        x_host = (O.uniform_complex(shape, seed) if dist == "uniform"
+                  else O.normal_complex(shape, seed)).astype(np.complex128 if prec == nv.F64
+                                                             else np.complex64)
+        x0 = torch.from_numpy(x_host.reshape(-1)).cuda()
+
+    def forms():
+        if name == "c2c64":
+            return [("per_stage", "c2c", "b200", False), ("grid_backend", "c2c", "b200grid", False)]
+        if name == "c2c1024":
+            return [("plain", "c2c", "b200", False), ("split_tc", "c2c", "b200", True)]
+        return [("grid_backend", "c2c", "b200grid", False)]
+
+    ref_full = None
+    ref_planes = None
+    if name == "c2c64":
+        ref_full = O.c2c_nd(x_host)  # the C oracle
+        out["oracle"] = "C oracle FP64 (full grid)"
+    elif name == "c2c4d":
+        ref_full = O.c2c_nd(x_host, -1, "scipy")
+        out["oracle"] = "scipy.fft FP64 (full grid)"
+    else:
+        plane = shape[1] * shape[2]
+        xv = x0.view(shape)
+        t0 = time.perf_counter()
+        ref_planes = O.c2c_planes(lambda a, b: xv[a:b].cpu().numpy(), shape[0], C2_PLANES)
+        out["oracle"] = (f"scipy FP64 planes X[k0,:,:], k0 in {list(C2_PLANES)} "
+                         f"({time.perf_counter() - t0:.1f} s on the host)")
+        del plane
+    for key, kind, backend, split in forms():
+        with _env_split_tc(split):
+            f = nv.ParaFaFT(kind, shape, prec, backend=backend)
+        grid = backend == "b200grid"
+        data = f.buffer() if grid else torch.zeros(f.required_size, dtype=ctype, device="cuda")
+        arg = None if grid else data
+        data[:n].copy_(x0)
+        f.forward(arg)
+        torch.cuda.synchronize()
+        if ref_full is not None:
+            rel = O.rel_l2(data[:n].cpu().numpy().reshape(shape), ref_full)
+        else:
+            yv = data[:n].view(shape)
+            got = np.stack([yv[k].cpu().numpy() for k in C2_PLANES])
+            rel = O.rel_l2(got, ref_planes)
+        f.backward(arg)
+        torch.cuda.synchronize()
+        rt = _rel_dev(data[:n] / n, x0)
+        data[:n].copy_(x0)
+        h = None if grid else f.handle()
+        stream = None
+        if h is not None:
+            stream = torch.cuda.Stream()
+            h.set_stream(stream.cuda_stream)
+        step = lambda: (f.forward(arg), f.backward(arg))
+        k = steps * (20 if n < (1 << 20) else 1)  # tiny grid: more steps
+        clocks = ClockSampler(gpu_index)
+        clocks.start()
+        if h is not None:
+            step()
+            h.reset_stats()
+        ms = _timed_steps(step, k, warmup, stream, clocks)
+        clk = clocks.stop()
+        entry = {"backend": (f"ParaFaFT_C2C<{len(shape)}, "
+                             + (f"B200GridBackend<{len(shape)}, " if grid else "B200Backend<")
+                             + ("double>>" if prec == nv.F64 else "float>>")),
+                 "ms": round(ms, 4), "steps": k,
+                 "hbm_frac": round(alg / (ms * 1e-3) / 1e9 / peak, 4),
+                 "gbps": round(alg / (ms * 1e-3) / 1e9, 1),
+                 "rel_l2_fwd": rel, "rel_l2_roundtrip": rt, "clocks": clk}
+        if h is not None:
+            st = h.stats()
+            entry["gpu_launches_per_step"] = round(st["kernel_launches"] / (k + warmup), 2)
+            entry["copies_per_step"] = round(st["copies_issued"] / (k + warmup), 2)
+        if split:
+            desc = f.handle().plan_describe(nv.KIND_C2C, 0).split()[0]
+            entry["row_kernel"] = desc
+        out[key] = entry
+        f.close()
         del data
         torch.cuda.empty_cache()
-        gen2 = torch.Generator(device="cuda").manual_seed(seed + 1)
-        line["grid_backend"] = time_grid_backend(
-            "c2c", shape, prec,
-            lambda b: b.copy_(torch.randn(b.numel(), generator=gen2, device="cuda", dtype=b.dtype)),
-            args.steps, args.warmup)
-        line["grid_backend"]["hbm_frac"] = round(
-            alg / (line["grid_backend"]["ms"] * 1e-3) / 1e9 / peak, 4)
+    if name == "c2c1024":
+        out["split_tc"]["speedup_vs_plain"] = round(out["plain"]["ms"] / out["split_tc"]["ms"], 3)
+        out["split_tc"]["error_vs_plain"] = round(out["split_tc"]["rel_l2_fwd"] /
+                                                 out["plain"]["rel_l2_fwd"], 3)
+    del x0
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_c2c_config(args):
+    line = {"metric": f"{args.config} C2C fwd+bwd ms", "unit": "ms", "n_gpus": 1,
+            "higher_is_better": False, "steps": args.steps, "warmup": args.warmup}
+    line.update(measure_c2c(args.config, args.steps, args.warmup))
     print(json.dumps(line), flush=True)
     return 0
 
@@ -475,31 +547,33 @@ def time_grid_backend(kind, shape, prec, fill, steps, warmup):
 UNEVEN_SIDES = [32, 48, 60, 64, 80, 96, 120, 128, 160]
 
 
-def run_uneven(args):
-    """256 independent R2C float32 grids of uneven sizes (each side drawn from
-    UNEVEN_SIDES with numpy.random.default_rng(seed)), Gaussian random fields
-    with P(k) ~ k^-3. Times forward+backward of all grids three ways, through
-    one ParaFaFT_R2C<3, B200Backend<float>> object per grid:
+def measure_uneven(grids, seed, steps, warmup, gpu_index=0):
+    """`grids` independent R2C float32 grids of uneven sizes (each side drawn
+    from UNEVEN_SIDES with numpy.random.default_rng(seed)), Gaussian random
+    fields with P(k) ~ k^-3, one ParaFaFT_R2C<3, B200Backend<float>> object per
+    grid. Forward+backward of all grids timed three ways:
       loop    the grids one after another (per-grid launches and syncs),
-      grouped one b200fft group: pass depth d of all grids in one persistent
-              launch (6 launches in all),
+      grouped one b200fft group: each dependency level of all grids launched
+              together (per-length launches side by side on several streams),
       graph   the grouped schedule captured once in a CUDA graph and replayed.
-    """
+    Every grid's forward output is checked against the FP64 oracle (scipy.fft)
+    and its round trip against its input."""
     import torch
     from parafaft_b200 import native as nv
     from oracle import oracle as O
-    torch.cuda.set_device(0)
-    rng = np.random.default_rng(args.seed)
-    shapes = [tuple(int(s) for s in rng.choice(UNEVEN_SIDES, 3)) for _ in range(args.grids)]
-    objs, devs, hosts = [], [], []
+    torch.cuda.set_device(gpu_index)
+    rng = np.random.default_rng(seed)
+    shapes = [tuple(int(s) for s in rng.choice(UNEVEN_SIDES, 3)) for _ in range(grids)]
+    objs, devs, hosts, xs = [], [], [], []
     alg = 0
     for i, shp in enumerate(shapes):
-        x = O.gaussian_random_field(shp, args.seed + 1 + i).astype(np.float32)
+        x = O.gaussian_random_field(shp, seed + 1 + i).astype(np.float32)
         f = nv.ParaFaFT("r2c", shp, nv.F32)
         buf = np.zeros(f.required_size, np.float32)
         p = O.pad_real(x, np.float32)
         buf[:p.size] = p
         objs.append(f)
+        xs.append(x)
         hosts.append(torch.from_numpy(buf))
         devs.append(torch.from_numpy(buf).cuda())
         nr = int(np.prod(shp))
@@ -507,25 +581,12 @@ def run_uneven(args):
         alg += 2 * (4 * nr + 40 * nc)  # R2C pass + two C2C passes, each direction
     dflt = torch.cuda.default_stream()
 
-    def timed(fn, steps):
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(dflt)
-        for _ in range(steps):
-            fn()
-        e1.record(dflt)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps
-
     def loop():
         for f, d in zip(objs, devs):
             f.forward(d)
             f.backward(d)
 
-    for _ in range(args.warmup):
-        loop()
-    loop_ms = timed(loop, args.steps)
+    loop_ms = _timed_steps(loop, steps, warmup, dflt)
     g = nv.Group([f.handle() for f in objs])
     g.begin()
     for f, d in zip(objs, devs):
@@ -533,43 +594,55 @@ def run_uneven(args):
         f.backward(d)
     g.end()
     g.sync()
-    for _ in range(args.warmup):
-        g.replay()
-    grouped_ms = timed(g.replay, args.steps)
+    grouped_ms = _timed_steps(g.replay, steps, warmup, dflt)
     g.capture()
-    for _ in range(args.warmup):
-        g.replay()
-    graph_ms = timed(g.replay, args.steps)
-    # correctness of one grouped round trip against the inputs
+    clocks = ClockSampler(gpu_index)
+    clocks.start()
+    graph_ms = _timed_steps(g.replay, steps, warmup, dflt, clocks)
+    clk = clocks.stop()
+    # forward of every grid (per-grid objects) against the FP64 oracle
+    fwd_errs = []
+    for f, d, h, x, shp in zip(objs, devs, hosts, xs, shapes):
+        d.copy_(h)
+        f.forward(d)
+        npad = shp[0] * shp[1] * 2 * (shp[2] // 2 + 1)
+        X = O.complex_view(d.cpu().numpy()[:npad], shp)
+        fwd_errs.append(O.rel_l2(X, O.r2c_nd(x.astype(np.float64), impl="scipy")))
+    # one grouped (graph) round trip of all grids against their inputs
     for d, h in zip(devs, hosts):
         d.copy_(h)
     g.replay()
     g.sync()
-    errs = []
-    for shp, d, h in zip(shapes, devs, hosts):
-        n = int(np.prod(shp))
+    rt_errs = []
+    for shp, d, x in zip(shapes, devs, xs):
         npad = shp[0] * shp[1] * 2 * (shp[2] // 2 + 1)
-        y = O.unpad_real(d.cpu().numpy()[:npad], shp) / n
-        x = O.unpad_real(h.numpy()[:npad], shp)
-        errs.append(O.rel_l2(y, x))
+        y = O.unpad_real(d.cpu().numpy()[:npad], shp) / x.size
+        rt_errs.append(O.rel_l2(y, x))
     stats = g.stats()
     peak, peak_kind = _peaks()
-    line = {
-        "metric": "256 uneven R2C f32 grids fwd+bwd ms", "value": round(graph_ms, 4),
-        "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "higher_is_better": False, "dtype": "f32",
-        "data": f"synthetic Gaussian random fields P(k)~k^-3, seed {args.seed}",
-        "config": {"workload": "256 independent ParaFaFT_R2C<3,float> grids, sides from "
-                               + str(UNEVEN_SIDES), "grids": args.grids,
-                   "total_points": int(sum(np.prod(s) for s in shapes))},
+    g.close()
+    for f in objs:
+        f.close()
+    return {
+        "workload": f"{grids} independent ParaFaFT_R2C<3, float> grids, sides from {UNEVEN_SIDES}",
+        "input": f"Gaussian random fields P(k)~k^-3, zero mean, seed {seed}",
+        "grids": grids, "total_points": int(sum(np.prod(s) for s in shapes)),
         "loop_ms": round(loop_ms, 4), "grouped_ms": round(grouped_ms, 4),
         "graph_ms": round(graph_ms, 4), "speedup_graph_vs_loop": round(loop_ms / graph_ms, 2),
         "alg_bytes": alg, "hbm_frac_graph": round(alg / (graph_ms * 1e-3) / 1e9 / peak, 4),
-        "peak_source": peak_kind, "max_rel_l2_roundtrip": max(errs),
-        "group": stats,
+        "peak_gbs": peak, "peak_source": peak_kind,
+        "oracle": "scipy.fft FP64 per grid",
+        "max_rel_l2_fwd": max(fwd_errs), "max_rel_l2_roundtrip": max(rt_errs),
+        "group": stats, "clocks": clk,
     }
+
+
+def run_uneven(args):
+    line = {"metric": "256 uneven R2C f32 grids fwd+bwd ms", "unit": "ms", "n_gpus": 1,
+            "higher_is_better": False, "steps": args.steps, "warmup": args.warmup}
+    line.update(measure_uneven(args.grids, args.seed, args.steps, args.warmup))
+    line["value"] = line["graph_ms"]
     print(json.dumps(line), flush=True)
-    g.close()
     return 0
 
 
@@ -809,6 +882,28 @@ def run_b200(args):
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], pg, "cuda")
 
+    # ---- the other configurations, each with its own oracle check and
+    #      roofline (one GPU only: at N > 1 the replicas run the headline alone)
+    configs = None
+    if world == 1 and not args.headline_only:
+        fft.close()
+        del dev, pinned, result_host
+        torch.cuda.empty_cache()
+        configs = {}
+        for key, fn in (("c0_c2c64_f64", lambda: measure_c2c("c2c64", args.steps, args.warmup, local)),
+                        ("c2_c2c1024_f32", lambda: measure_c2c("c2c1024", max(4, args.steps // 2),
+                                                               args.warmup, local)),
+                        ("c3_uneven256_r2c_f32", lambda: measure_uneven(args.grids, args.seed,
+                                                                        args.steps, args.warmup, local)),
+                        ("c4_c2c4d_f64", lambda: measure_c2c("c2c4d", args.steps, args.warmup, local))):
+            t0 = time.perf_counter()
+            try:
+                configs[key] = fn()
+            except Exception as e:  # reported, never silently dropped
+                configs[key] = {"error": f"{type(e).__name__}: {e}"}
+            configs[key]["wall_s"] = round(time.perf_counter() - t0, 1)
+            torch.cuda.empty_cache()
+
     if rank == 0:
         cpu_ms, cpu_n, cores = time_cpu(host_buf, budget_s=args.cpu_budget, max_steps=8)
         nbytes = host_buf.nbytes
@@ -839,6 +934,7 @@ def run_b200(args):
             "cufft_backend_ms": cufft_ms if isinstance(cufft_ms, str) else round(cufft_ms, 4),
             "split_tc": split,
             "grid_backend": grid,
+            "configs": configs if configs is not None else "headline only (N > 1 replicas or --headline-only)",
             "gpu_launches": int(launches),
             "clocks": clk,
             "cpu_baseline": {"value": round(cpu_ms, 1), "unit": "ms", "cores": cores, "kind": "port",
@@ -846,7 +942,8 @@ def run_b200(args):
                                        f"(FFTWBackend<float> stand-in: libfftw3f absent)"},
         }
         print(json.dumps(line), flush=True)
-    fft.close()
+    if configs is None:
+        fft.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -867,6 +964,8 @@ def main():
                     choices=["r2c512", "uneven256", "c2c64", "c2c1024", "c2c4d"],
                     help="r2c512: the headline 512^3 R2C (default); uneven256: 256 "
                          "uneven grids; c2c64 / c2c1024 / c2c4d: the C2C configurations")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="time the 512^3 headline alone, without the other configurations")
     ap.add_argument("--grids", type=int, default=256)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--single-pass", default=None, metavar="KIND,LENGTH,LAYOUT,BATCH",
