@@ -443,6 +443,21 @@ struct b200fft_group_s {
   std::vector<cudaStream_t> aux;
   std::vector<cudaEvent_t> aux_done;
   cudaEvent_t level_start = nullptr;
+  // The dependency-scheduled form (fft_sched.cu, B200FFT_GROUP_SCHEDULE=1):
+  // when every recorded pass has a tile in the schedule kernel, the whole
+  // schedule is one persistent launch over a (pass, tile) work list instead
+  // of the level steps.
+  bool sched = false;
+  std::vector<SchedPass> spasses;
+  std::vector<int2> sorder;
+  SchedPass *d_spasses = nullptr;
+  int2 *d_sorder = nullptr;
+  unsigned *d_sdone = nullptr;              // per-pass tile counters
+  unsigned long long *d_sclaim = nullptr;   // next work item
+  unsigned *d_sfault = nullptr;             // a wait ran out of time
+  int sgrid = 0;
+  long long sbytes = 0;
+  unsigned long long swait_ns = 1000000000ull;
 };
 
 namespace {
@@ -1632,6 +1647,22 @@ void group_free_schedule(G *g) {
     if (g->level_start)
       cudaEventDestroy(g->level_start);
   }
+  if (!g->record_only) {
+    if (g->d_spasses)
+      cudaFree(g->d_spasses);
+    if (g->d_sorder)
+      cudaFree(g->d_sorder);
+    if (g->d_sdone)
+      cudaFree(g->d_sdone);
+  }
+  g->sched = false;
+  g->spasses.clear();
+  g->sorder.clear();
+  g->d_spasses = nullptr;
+  g->d_sorder = nullptr;
+  g->d_sdone = nullptr;
+  g->d_sclaim = nullptr;
+  g->sbytes = 0;
   g->aux.clear();
   g->aux_done.clear();
   g->level_start = nullptr;
@@ -1650,9 +1681,175 @@ int sm_count_current() {
   return n;
 }
 
+// Elements (complex) a pass spans on one side, from its first element to its
+// last: the last point of the last transform of the last slab.
+long long pass_extent(const PassArgs &a, int points, bool in) {
+  const long long slabs = a.batch > 0 ? (a.total + a.batch - 1) / a.batch : 1;
+  const long long dist = in ? a.idist : a.odist;
+  const long long stride = in ? a.istride : a.ostride;
+  const long long slab = in ? a.islab : a.oslab;
+  return (slabs - 1) * slab + (std::min(a.total, a.batch) - 1) * dist +
+         static_cast<long long>(points - 1) * stride + 1;
+}
+
+// The dependency-scheduled form of a group (fft_sched.cu), chosen with
+// B200FFT_GROUP_SCHEDULE=1. It applies when every member is FP32, every
+// recorded operation is a pass whose specialised tile the schedule kernel
+// carries, and no two members touch the same memory (grids are then
+// independent, so only each grid's own passes order one another). Returns
+// false (and leaves g untouched) where it does not apply. It is not the
+// default: on 256 uneven grids the one persistent launch took 2.6 ms against
+// 2.2 ms for the per-level launches of specialised kernels (its tiles run
+// under one register budget and one instruction stream for all lengths).
+bool sched_build(G *g, int *rc) {
+  *rc = B200FFT_SUCCESS;
+  if (!env_flag("B200FFT_GROUP_SCHEDULE"))
+    return false;
+  struct Span {
+    uintptr_t lo, hi;
+  };
+  std::vector<Span> spans; // every member's memory, as disjoint intervals
+  std::vector<SchedPass> passes;
+  std::vector<std::pair<long long, int>> keyed; // (order key, pass)
+  // a pass is listed `lag` keys after its dependency; lag >= 1 keeps every
+  // pass after the pass it waits for
+  long long lag = 2;
+  if (const char *v = std::getenv("B200FFT_SCHED_LAG"))
+    lag = std::max(1ll, std::atoll(v));
+
+  long long bytes = 0;
+  for (size_t hi = 0; hi < g->handles.size(); ++hi) {
+    H *h = g->handles[hi];
+    if (h->prec != B200FFT_F32 || h->recs.empty())
+      return false;
+    std::vector<Span> own; // this member's pass sides
+    int prev = -1;
+    for (size_t k = 0; k < h->recs.size(); ++k) {
+      const RecOp &op = h->recs[k];
+      if (op.type != RecOp::PASS)
+        return false;
+      const Plan &p = op.plan;
+      Choice sc;
+      if (h->force_generic ||
+          choose_kernel(h->prec, p.kind, p.len, p.batch, p.stride, p.dist, false, &sc, 0) !=
+              B200FFT_SUCCESS ||
+          sc.family != 0)
+        return false;
+      const int spec = sched_spec_index(p.kind, sc.col, op.dir == B200FFT_FORWARD, sc.L);
+      if (spec < 0)
+        return false;
+      SchedPass q{};
+      q.a = pass_args(p, 0, op.in, op.out, op.tw, op.slabs, op.slab);
+      q.spec = spec;
+      const long long tb = sched_tile_transforms(spec);
+      const long long nt = (q.a.total + tb - 1) / tb;
+      if (nt <= 0 || nt > INT_MAX)
+        return false;
+      q.ntiles = static_cast<unsigned>(nt);
+      q.dep = prev;
+      q.need = prev >= 0 ? passes[static_cast<size_t>(prev)].ntiles : 0;
+      const size_t cs = h->csize();
+      const uintptr_t in0 = reinterpret_cast<uintptr_t>(q.a.in);
+      const uintptr_t out0 = reinterpret_cast<uintptr_t>(q.a.out);
+      // points per transform on each side: R2C rows read L complex (2L reals)
+      // and write L+1, C2R rows the reverse
+      const int pin = p.kind == KIND_C2R ? sc.L + 1 : sc.L;
+      const int pout = p.kind == KIND_R2C ? sc.L + 1 : sc.L;
+      const uintptr_t in1 = in0 + cs * static_cast<uintptr_t>(pass_extent(q.a, pin, true));
+      const uintptr_t out1 = out0 + cs * static_cast<uintptr_t>(pass_extent(q.a, pout, false));
+      own.push_back({in0, in1});
+      own.push_back({out0, out1});
+      bytes += pass_bytes(h, p, q.a.total);
+      prev = static_cast<int>(passes.size());
+      keyed.push_back({static_cast<long long>(hi) + lag * static_cast<long long>(k), prev});
+      passes.push_back(q);
+    }
+    // union of this member's intervals (its passes share its buffers)
+    std::sort(own.begin(), own.end(), [](const Span &a, const Span &b) { return a.lo < b.lo; });
+    const size_t first = spans.size();
+    for (const Span &x : own) {
+      if (spans.size() > first && x.lo <= spans.back().hi)
+        spans.back().hi = std::max(spans.back().hi, x.hi);
+      else
+        spans.push_back(x);
+    }
+  }
+  // members' intervals must not meet: sorted by start, each begins at or
+  // after the furthest end before it (a member's own intervals are disjoint)
+  std::sort(spans.begin(), spans.end(), [](const Span &a, const Span &b) { return a.lo < b.lo; });
+  uintptr_t reach = 0;
+  for (const Span &x : spans) {
+    if (x.lo < reach)
+      return false; // members share memory: keep the level barriers
+    reach = std::max(reach, x.hi);
+  }
+  // list order: by key; within a key, later passes (of grids further ahead)
+  // first, their dependencies being the oldest
+  std::stable_sort(keyed.begin(), keyed.end(), [&](const auto &a, const auto &b) {
+    if (a.first != b.first)
+      return a.first < b.first;
+    return a.second > b.second;
+  });
+  std::vector<int2> order;
+  for (const auto &kp : keyed)
+    for (unsigned t = 0; t < passes[static_cast<size_t>(kp.second)].ntiles; ++t)
+      order.push_back(make_int2(kp.second, static_cast<int>(t)));
+  if (env_flag("B200FFT_SCHED_STALL_TEST")) {
+    // test hook: the last dependent pass waits for one tile more than exist,
+    // so its waits run out (bounded, 20 ms) and the fault path is taken
+    for (size_t i = passes.size(); i-- > 0;)
+      if (passes[i].dep >= 0) {
+        passes[i].need += 1;
+        break;
+      }
+    g->swait_ns = 20000000ull;
+  } else {
+    g->swait_ns = 1000000000ull;
+  }
+  g->spasses = std::move(passes);
+  g->sorder = std::move(order);
+  g->sbytes = bytes;
+  g->sched = true;
+  if (g->record_only)
+    return true;
+  const size_t np = g->spasses.size();
+  // counters: np per-pass words, padding to 8 bytes, the claim word, the fault word
+  const size_t claim_off = (np * sizeof(unsigned) + 7) & ~size_t(7);
+  const size_t cbytes = claim_off + sizeof(unsigned long long) + sizeof(unsigned);
+  cudaError_t e = cudaMalloc(&g->d_spasses, np * sizeof(SchedPass));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&g->d_sorder, g->sorder.size() * sizeof(int2));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&g->d_sdone, cbytes);
+  if (e == cudaSuccess) {
+    g->d_sclaim = reinterpret_cast<unsigned long long *>(
+        reinterpret_cast<char *>(g->d_sdone) + claim_off);
+    g->d_sfault = reinterpret_cast<unsigned *>(g->d_sclaim + 1);
+    e = cudaMemset(g->d_sdone, 0, cbytes);
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpy(g->d_spasses, g->spasses.data(), np * sizeof(SchedPass),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(g->d_sorder, g->sorder.data(), g->sorder.size() * sizeof(int2),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = sched_grid(&g->sgrid);
+  if (e != cudaSuccess) {
+    *rc = cuda_fail(e, "group schedule upload");
+    return true;
+  }
+  return true;
+}
+
 // Build the steps of the schedule from the members' recordings.
 int group_build(G *g) {
   group_free_schedule(g);
+  {
+    int rc = B200FFT_SUCCESS;
+    if (sched_build(g, &rc))
+      return rc;
+  }
   size_t depth = 0;
   for (H *h : g->handles)
     depth = std::max(depth, h->recs.size());
@@ -1836,6 +2033,31 @@ int group_build(G *g) {
 
 int group_run(G *g) {
   g->stats.exec_calls++;
+  if (g->sched) {
+    g->stats.kernel_launches++;
+    g->stats.bytes_transformed += static_cast<uint64_t>(g->sbytes);
+    if (g->record_only)
+      return B200FFT_SUCCESS;
+    cudaGetLastError();
+    // zero the pass counters and the claim word (not the fault word)
+    const size_t claim_end = reinterpret_cast<char *>(g->d_sclaim + 1) -
+                             reinterpret_cast<char *>(g->d_sdone);
+    cudaError_t e = cudaMemsetAsync(g->d_sdone, 0, claim_end, g->stream);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "schedule counter reset");
+    SchedArgs a{};
+    a.passes = g->d_spasses;
+    a.items = g->d_sorder;
+    a.nitems = static_cast<long long>(g->sorder.size());
+    a.done = g->d_sdone;
+    a.claim = g->d_sclaim;
+    a.fault = g->d_sfault;
+    a.wait_ns = g->swait_ns;
+    e = launch_sched(a, g->sgrid, g->stream);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "schedule kernel launch");
+    return B200FFT_SUCCESS;
+  }
   for (GroupStep &s : g->steps) {
     if (s.type == GroupStep::PASSES || s.type == GroupStep::STATIC ||
         s.type == GroupStep::SINGLE) {
@@ -2072,6 +2294,18 @@ int b200fft_group_sync(b200fft_group g) {
   cudaError_t e = cudaStreamSynchronize(g->stream);
   if (e != cudaSuccess)
     return cuda_fail(e, "cudaStreamSynchronize (group)");
+  if (g->sched && g->d_sfault) {
+    unsigned fault = 0;
+    e = cudaMemcpy(&fault, g->d_sfault, sizeof(fault), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && fault)
+      e = cudaMemset(g->d_sfault, 0, sizeof(unsigned));
+    if (e != cudaSuccess)
+      return cuda_fail(e, "schedule fault word");
+    if (fault)
+      return fail(B200FFT_ERR_DEVICE_STATUS,
+                  "b200fft: the group schedule kernel gave up waiting for a pass "
+                  "(results of that run are invalid)");
+  }
   return B200FFT_SUCCESS;
 }
 
@@ -2079,7 +2313,7 @@ int b200fft_group_stats(b200fft_group g, b200fft_stats *out) {
   if (g == nullptr || out == nullptr)
     return fail(B200FFT_ERR_INVALID_ARG, "b200fft_group_stats: null argument");
   *out = g->stats;
-  size_t passes = 0;
+  size_t passes = g->sched ? g->spasses.size() : 0;
   for (const GroupStep &s : g->steps)
     passes += s.items.size() + s.sitems.size();
   out->exec_calls = g->stats.exec_calls;

@@ -68,6 +68,36 @@ cudaError_t launch_generic_group(bool f64, int kind, bool col, bool fwd, const G
                                  cudaStream_t st);
 constexpr size_t kGenericSmemLimit = 200 * 1024;
 
+// Dependency-scheduled persistent pass kernel (fft_sched.cu): the passes of
+// a group of independent grids in one launch. Pass `dep` (whole pass) must be
+// done before any tile of this pass starts; `spec` picks the specialised tile
+// code (sched_spec_index).
+constexpr int kSchedThreads = 256;
+struct SchedPass {
+  PassArgs a;
+  int spec;      // specialised tile code of the pass
+  int dep;       // pass this one waits for (-1: none)
+  unsigned need; // tiles of `dep` (all of them)
+  unsigned ntiles;
+};
+struct SchedArgs {
+  const SchedPass *passes;
+  const int2 *items;         // (pass, tile) in claim order
+  long long nitems;
+  unsigned *done;            // finished tiles per pass, zeroed before each run
+  unsigned long long *claim; // next item, zeroed before each run
+  unsigned *fault;           // set when a dependency wait ran out of time
+  unsigned long long wait_ns; // bound of one wait
+};
+// Index of the specialised tile for (kind, layout, direction, length), or -1
+// when the schedule kernel does not carry it; transforms per tile of a spec.
+int sched_spec_index(int kind, bool col, bool fwd, int L);
+int sched_tile_transforms(int spec);
+size_t sched_smem_bytes();
+// CTAs of a persistent launch on the current device (all resident at once).
+cudaError_t sched_grid(int *grid);
+cudaError_t launch_sched(const SchedArgs &s, int grid, cudaStream_t st);
+
 // Entries of the twiddle table of top length n: a pyramid T_n, T_{n/2}, ...,
 // T_1 for powers of two (2n - 1 entries), else T_n alone.
 int twiddle_table_entries(int n);

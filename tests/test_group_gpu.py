@@ -3,7 +3,9 @@
 Each grid is its own ParaFaFT_R2C<3, B200Backend<float>> object; their
 forward+backward passes are recorded in one group and launched together, then
 replayed, then replayed from a CUDA graph. Every run must equal the per-grid
-result and the FP64 oracle.
+result and the FP64 oracle. Both forms of a group run: the per-level launches
+(default) and the dependency-scheduled persistent launch
+(B200FFT_GROUP_SCHEDULE=1).
 """
 import numpy as np
 import pytest
@@ -35,7 +37,16 @@ def _launches_per_direction(shapes):
     return sum(len({s[a] for s in shapes}) for a in range(3))
 
 
-def test_group_forward_matches_oracle_and_per_grid():
+@pytest.fixture(params=["schedule", "levels"])
+def form(request, monkeypatch):
+    if request.param == "schedule":
+        monkeypatch.setenv("B200FFT_GROUP_SCHEDULE", "1")
+    else:
+        monkeypatch.delenv("B200FFT_GROUP_SCHEDULE", raising=False)
+    return request.param
+
+
+def test_group_forward_matches_oracle_and_per_grid(form):
     _drivers_or_skip()
     shapes = _grids(12, 5)
     objs, devs, xs = [], [], []
@@ -54,15 +65,16 @@ def test_group_forward_matches_oracle_and_per_grid():
         f.forward(d)
     g.end()
     g.sync()
-    # one grouped launch per pass depth and kernel length
-    assert g.stats()["kernel_launches"] == _launches_per_direction(shapes)
+    # one persistent launch, or one grouped launch per pass depth and length
+    assert g.stats()["kernel_launches"] == (1 if form == "schedule"
+                                            else _launches_per_direction(shapes))
     for shp, x, d in zip(shapes, xs, devs):
         nc = shp[-1] // 2 + 1
         X = to_host(d)[:2 * shp[0] * shp[1] * nc].view(np.complex64).reshape(shp[0], shp[1], nc)
         assert O.rel_l2(X, O.r2c_nd(x.astype(np.float64))) < REL_F32, shp
 
 
-def test_group_roundtrip_replay_and_graph():
+def test_group_roundtrip_replay_and_graph(form):
     _drivers_or_skip()
     shapes = _grids(20, 9)
     objs, devs, xs = [], [], []
@@ -104,10 +116,60 @@ def test_group_roundtrip_replay_and_graph():
     check(1)
     st = g.stats()
     runs = 2  # the run at end() and the replay (graph replays are not counted)
-    assert st["kernel_launches"] == runs * 2 * _launches_per_direction(shapes)
+    assert st["kernel_launches"] == runs * (1 if form == "schedule"
+                                            else 2 * _launches_per_direction(shapes))
     assert st["passes_per_run"] == 20 * 6
     g.close()
     # members work on their own again after the group is gone
     for f, d in zip(objs[:2], devs[:2]):
         f.forward(d)
         f.backward(d)
+
+
+def test_schedule_wait_bound_reports_device_status(monkeypatch):
+    """The schedule kernel's dependency waits are bounded: with the test hook
+    one pass waits for a tile that never comes, the wait runs out (20 ms), the
+    kernel sets its fault word and returns, and b200fft_group_sync reports
+    DEVICE_STATUS. The context stays usable: a group built afterwards is
+    correct."""
+    _drivers_or_skip()
+    monkeypatch.setenv("B200FFT_GROUP_SCHEDULE", "1")
+    shapes = _grids(6, 21)
+
+    def build():
+        objs, devs, xs = [], [], []
+        for i, shp in enumerate(shapes):
+            x = O.normal_real(shp, 50 + i).astype(np.float32)
+            f = nv.ParaFaFT("r2c", shp, nv.F32)
+            buf = np.zeros(f.required_size, np.float32)
+            p = O.pad_real(x, np.float32)
+            buf[:p.size] = p
+            objs.append(f)
+            devs.append(to_dev(buf))
+            xs.append(x)
+        return objs, devs, xs
+
+    objs, devs, _ = build()
+    monkeypatch.setenv("B200FFT_SCHED_STALL_TEST", "1")
+    g = nv.Group([f.handle() for f in objs])
+    g.begin()
+    for f, d in zip(objs, devs):
+        f.forward(d)
+    g.end()
+    with pytest.raises(nv.B200FFTError) as ei:
+        g.sync()
+    assert ei.value.code == -7  # B200FFT_ERR_DEVICE_STATUS
+    g.close()
+    monkeypatch.delenv("B200FFT_SCHED_STALL_TEST")
+    objs, devs, xs = build()
+    g = nv.Group([f.handle() for f in objs])
+    g.begin()
+    for f, d in zip(objs, devs):
+        f.forward(d)
+    g.end()
+    g.sync()
+    for shp, x, d in zip(shapes, xs, devs):
+        nc = shp[-1] // 2 + 1
+        X = to_host(d)[:2 * shp[0] * shp[1] * nc].view(np.complex64).reshape(shp[0], shp[1], nc)
+        assert O.rel_l2(X, O.r2c_nd(x.astype(np.float64))) < REL_F32, shp
+    g.close()

@@ -207,11 +207,17 @@ print(st["kernel_launches"], st["copies_issued"])
 
 
 @pytest.mark.skipif(not _drivers_built(), reason="ParaFaFT drivers not built")
-def test_group_schedules_many_grids_per_depth_and_length():
+@pytest.mark.parametrize("form", ["schedule", "levels"])
+def test_group_schedules_many_grids_per_depth_and_length(form, monkeypatch):
     """256 ParaFaFT_R2C<3> objects of uneven sizes, forward+backward recorded in
-    one group: at each of the 6 pass depths one grouped launch per distinct
-    kernel length (every side here has a specialised kernel), 256*6 passes,
-    no copies."""
+    one group, 256*6 passes, no copies. Default: at each of the 6 pass depths
+    one grouped launch per distinct kernel length (every side here has a
+    specialised kernel). With B200FFT_GROUP_SCHEDULE=1: the dependency-
+    scheduled form, one persistent launch for the whole schedule."""
+    if form == "schedule":
+        monkeypatch.setenv("B200FFT_GROUP_SCHEDULE", "1")
+    else:
+        monkeypatch.delenv("B200FFT_GROUP_SCHEDULE", raising=False)
     out = _run_record(r'''
 import ctypes as C, numpy as np
 from parafaft_b200 import native as nv
@@ -235,8 +241,33 @@ expect = 2 * (len({s[2] for s in shapes}) + len({s[1] for s in shapes}) + len({s
 print(st["kernel_launches"], st["passes_per_run"], st["copies_issued"], expect)
 ''')
     launches, passes, copies, expect = out.split()
-    assert launches == expect and passes == str(256 * 6) and copies == "0"
-    assert int(launches) <= 6 * 9
+    assert passes == str(256 * 6) and copies == "0"
+    if form == "levels":
+        assert launches == expect and int(launches) <= 6 * 9
+    else:
+        assert launches == "1"
+
+
+@pytest.mark.skipif(not _drivers_built(), reason="ParaFaFT drivers not built")
+def test_group_members_sharing_memory_keep_level_barriers(monkeypatch):
+    """Two grids transformed in the same buffer are not independent: the
+    group keeps its per-level launches even when the dependency schedule is
+    asked for (it orders only each grid's own passes)."""
+    monkeypatch.setenv("B200FFT_GROUP_SCHEDULE", "1")
+    out = _run_record(r'''
+import ctypes as C
+from parafaft_b200 import native as nv
+a = nv.ParaFaFT("r2c", (32, 48, 60), nv.F32)
+b = nv.ParaFaFT("r2c", (32, 48, 60), nv.F32)
+buf = C.c_void_p(); nv.check(nv.engine().b200fft_alloc(a.required_size * 4, C.byref(buf)))
+g = nv.Group([a.handle(), b.handle()])
+g.begin()
+a.forward(buf.value)
+b.forward(buf.value)
+g.end()
+print(g.stats()["kernel_launches"])
+''')
+    assert int(out.split()[0]) > 1
 
 
 def test_wisdom_roundtrip_and_plan_choice(tmp_path):
