@@ -555,7 +555,10 @@ def measure_uneven(grids, seed, steps, warmup, gpu_index=0):
       loop    the grids one after another (per-grid launches and syncs),
       grouped one b200fft group: each dependency level of all grids launched
               together (per-length launches side by side on several streams),
-      graph   the grouped schedule captured once in a CUDA graph and replayed.
+      graph   the grouped schedule captured once in a CUDA graph and replayed;
+      schedule (graph) the dependency-scheduled form: one persistent launch
+              walking a work list of (pass, tile) items, each grid's passes
+              waiting only for that grid's previous pass.
     Every grid's forward output is checked against the FP64 oracle (scipy.fft)
     and its round trip against its input."""
     import torch
@@ -587,13 +590,34 @@ def measure_uneven(grids, seed, steps, warmup, gpu_index=0):
             f.backward(d)
 
     loop_ms = _timed_steps(loop, steps, warmup, dflt)
-    g = nv.Group([f.handle() for f in objs])
-    g.begin()
-    for f, d in zip(objs, devs):
-        f.forward(d)
-        f.backward(d)
-    g.end()
-    g.sync()
+
+    def make_group(schedule):
+        old = os.environ.pop("B200FFT_GROUP_SCHEDULE", None)
+        if schedule:
+            os.environ["B200FFT_GROUP_SCHEDULE"] = "1"
+        try:
+            grp = nv.Group([f.handle() for f in objs])
+            grp.begin()
+            for f, d in zip(objs, devs):
+                f.forward(d)
+                f.backward(d)
+            grp.end()
+            grp.sync()
+        finally:
+            os.environ.pop("B200FFT_GROUP_SCHEDULE", None)
+            if old is not None:
+                os.environ["B200FFT_GROUP_SCHEDULE"] = old
+        return grp
+
+    # the dependency-scheduled form (one persistent launch over a work list of
+    # (pass, tile) items), as a CUDA graph
+    gs = make_group(True)
+    gs.capture()
+    sched_graph_ms = _timed_steps(gs.replay, steps, warmup, dflt)
+    sched_stats = gs.stats()
+    gs.close()
+    # the default form: per-level launches of the specialised kernels
+    g = make_group(False)
     grouped_ms = _timed_steps(g.replay, steps, warmup, dflt)
     g.capture()
     clocks = ClockSampler(gpu_index)
@@ -629,6 +653,8 @@ def measure_uneven(grids, seed, steps, warmup, gpu_index=0):
         "grids": grids, "total_points": int(sum(np.prod(s) for s in shapes)),
         "loop_ms": round(loop_ms, 4), "grouped_ms": round(grouped_ms, 4),
         "graph_ms": round(graph_ms, 4), "speedup_graph_vs_loop": round(loop_ms / graph_ms, 2),
+        "schedule_graph_ms": round(sched_graph_ms, 4),
+        "schedule_launches_per_run": sched_stats["kernel_launches"] // max(1, sched_stats["runs"]),
         "alg_bytes": alg, "hbm_frac_graph": round(alg / (graph_ms * 1e-3) / 1e9 / peak, 4),
         "peak_gbs": peak, "peak_source": peak_kind,
         "oracle": "scipy.fft FP64 per grid",
@@ -809,16 +835,23 @@ def run_b200(args):
                                       for _ in range(NBUF - 1))
     s_up, s_down = torch.cuda.Stream(), torch.cuda.Stream()
     done_down = [torch.cuda.Event() for _ in range(NBUF)]
+    up_done = [torch.cuda.Event() for _ in range(NBUF)]
 
-    def e2e_step(i):
+    # forward()/backward() return only when the transform is done (ParaFaFT
+    # calls sync()), so step i+1's upload is issued before step i's transform:
+    # the upload then runs during the transform and both PCIe directions stay
+    # busy back to back
+    def upload(i):
         k = i % NBUF
-        d = bufs[k]
         s_up.wait_event(done_down[k])          # the buffer's previous result is out
         with torch.cuda.stream(s_up):
-            d.copy_(host_in[k], non_blocking=True)
-        up = torch.cuda.Event()
-        up.record(s_up)
-        stream.wait_event(up)
+            bufs[k].copy_(host_in[k], non_blocking=True)
+        up_done[k].record(s_up)
+
+    def transform_and_download(i):
+        k = i % NBUF
+        d = bufs[k]
+        stream.wait_event(up_done[k])
         fft.forward(d)
         fft.backward(d)
         comp = torch.cuda.Event()
@@ -828,18 +861,23 @@ def run_b200(args):
             host_out[k].copy_(d, non_blocking=True)
         done_down[k].record(s_down)
 
+    def e2e_run(n):
+        upload(0)
+        for i in range(n):
+            if i + 1 < n:
+                upload(i + 1)
+            transform_and_download(i)
+
     for k in range(NBUF):
         done_down[k].record(s_down)
-    for i in range(max(NBUF, args.warmup)):
-        e2e_step(i)
+    e2e_run(max(NBUF, args.warmup))
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
     e2.record(s_up)
-    for i in range(args.steps):
-        e2e_step(i)
+    e2e_run(args.steps)
     e3.record(s_down)
     torch.cuda.synchronize()
     e2e_ms = e2.elapsed_time(e3) / args.steps
@@ -930,7 +968,7 @@ def run_b200(args):
             "kernels": kernels,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes,
-                    "pipeline": "three device buffers; step i+1's upload, step i's transform and step i-1's download overlap"},
+                    "pipeline": "three device buffers; step i+1's upload (issued before step i's transform), step i's transform and step i-1's download overlap"},
             "cufft_backend_ms": cufft_ms if isinstance(cufft_ms, str) else round(cufft_ms, 4),
             "split_tc": split,
             "grid_backend": grid,

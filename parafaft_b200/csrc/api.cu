@@ -243,13 +243,19 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
       (kind == KIND_C2C || (!odd && stride == 1 && dist % 2 == 0 && L <= 2048));
   if (static_ok) {
     int var = default_variant(csize, L, ch.col, stride);
-    if (const char *v = std::getenv("B200FFT_VARIANT"))
-      if (v[0] >= '0' && v[0] < '0' + kStaticVariants && v[1] == '\0')
-        var = v[0] - '0';
+    if (const char *v = std::getenv("B200FFT_VARIANT")) {
+      char *end = nullptr;
+      const long ev = std::strtol(v, &end, 10);
+      if (end != v && *end == '\0' && ev >= 0 && ev < kStaticVariants)
+        var = static_cast<int>(ev);
+    }
     if (variant >= 0 && variant < kStaticVariants)
       var = variant;
     if (!is_pow2(L) && !(ch.col && var == 1))
       var = 0; // mixed-radix lengths: the full tile, or the half tile for columns
+    if (var == kVariantPair &&
+        !(ch.col && kind == KIND_C2C && csize == 8 && colpair_length_ok(L)))
+      var = default_variant(csize, L, ch.col, stride); // the pair tile does not apply
     const CfgS c = cfg_static(csize, L, ch.col, var);
     ch.variant = var;
     ch.family = 0;
@@ -825,6 +831,16 @@ cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
   if (p.ch.family == 0) {
     if (p.kind == KIND_C2C) {
       int var = column_tile_for(h, p, a.total);
+      // FP32 512-point columns whose neighbouring transforms sit side by side
+      // on 16-byte aligned rows (the first axis of a grid) take the pair tile
+      // by default: 16-byte loads, stores and exchanges (512^3 first-axis
+      // pass 0.212 -> 0.195 ms); odd point strides keep the one-transform
+      // tile (the pair tile's 8-byte form was slower there, 0.237 vs 0.225 ms)
+      if (var == 5 && h->plan_flag == B200FFT_PLAN_ESTIMATE && !f64 && p.ch.col &&
+          p.ch.L == 512 && colpair_vec_ok(a))
+        var = kVariantPair;
+      if (var == kVariantPair && !f64 && p.ch.col && colpair_length_ok(p.ch.L))
+        return launch_colpair_c2c_f32(p.ch.L, fwd, a, h->stream);
       if (var == kVariantTma || var == kVariantTma + 1) {
         if (!f64 && p.ch.col && tma_col_ok(p.ch.L, a)) {
           h->used_tma = true;
@@ -1002,8 +1018,8 @@ int autotune(H *h, Plan &p) {
   std::vector<std::pair<int, int>> cands; // (family, variant)
   if (p.ch.family == 0) {
     if (p.ch.col) {
-      const int meas[] = {0, 3, 5, 8};
-      const int pat[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9};
+      const int meas[] = {0, 3, 5, 8, 10};
+      const int pat[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10};
       if (rigor >= B200FFT_PLAN_PATIENT)
         for (int v : pat) cands.push_back({0, v});
       else
@@ -1118,9 +1134,13 @@ int exec_real(H *h, Plan &p, int kind, void *ptr) {
   }
   char *cp = static_cast<char *>(ptr);
   const size_t span = real_span_bytes(h, p);
+  // fold a held copy only into contiguous padded rows (no gaps the pass
+  // would skip; a C2R pass leaves each row's two pad reals unspecified, as
+  // an in-place C2R does)
+  const bool dense = p.stride == 1 && p.dist == 2 * (p.len / 2 + 1);
   bool fused = false;
   if (h->copy.active) {
-    if (copy_covers(h, cp, span))
+    if (dense && copy_covers(h, cp, span))
       fused = true;
     else
       B2_TRY(flush_copy(h));
@@ -1289,9 +1309,14 @@ int b200fft_exec_c2c(b200fft_handle h, int stage, int direction, void *data) {
   const size_t slab_bytes = lead > 1 ? static_cast<size_t>(p.len) * p.batch * h->csize()
                                      : c2c_span_bytes(h, p);
   const size_t region = static_cast<size_t>(lead) * slab_bytes;
+  // A held copy folds into the pass only when the pass writes every element
+  // of its region (no gaps between point rows or transforms): elements a
+  // pass skips would otherwise miss their copy.
+  const bool dense = lead > 1 || static_cast<size_t>(p.len) * static_cast<size_t>(p.batch) *
+                                         h->csize() == slab_bytes;
   bool fused = false;
   if (h->copy.active) {
-    if (copy_covers(h, cp, region))
+    if (dense && copy_covers(h, cp, region))
       fused = true;
     else
       B2_TRY(flush_copy(h));

@@ -363,9 +363,14 @@ struct CfgS {
 //       rows): persistent CTAs of 512 threads stream 64 KiB tiles through a
 //       ring of three shared-memory buffers filled by bulk tensor copies;
 //   9 = the same on 1024 threads per CTA.
-// Where a TMA variant does not apply, the plan's default tile runs instead.
-constexpr int kStaticVariants = 10;
+//  10 = pair-column tile (FP32, 256/512/1024 points): 512 (1024) threads, two
+//       neighbouring transforms per thread, 16-byte shared-memory exchanges
+//       and twiddles shared by the pair (fft_colpair.cuh).
+// Where a TMA or pair variant does not apply, the plan's default tile runs
+// instead.
+constexpr int kStaticVariants = 11;
 constexpr int kVariantTma = 8;
+constexpr int kVariantPair = 10;
 constexpr int kVariantStaged = 4;
 constexpr int kVariantPipelined = 6;
 
@@ -393,6 +398,14 @@ constexpr CfgS cfg_static(int esize, int L, bool col, int variant = 0) {
     const int P = Pe > 0 ? Pe : ce_min(NT, floor_pow2(ce_max(1, L / 8)));
     return CfgS{NT, NT / P, P, (L + P - 1) / P};
   }
+  if (col && variant == 10 && esize == 8 && (L == 256 || L == 512 || L == 1024)) {
+    // pair-column tile: TB/2 transform pairs, 8 points of each per thread
+    const int TB = L == 256 ? 32 : 16;
+    const int nt = L == 1024 ? 1024 : 512;
+    return CfgS{nt, TB, nt / (TB / 2), L / (nt / (TB / 2))};
+  }
+  if (variant == 10)
+    variant = 5; // the pair tile's shape where it does not apply
   const int NT = (col && (variant == 7 || variant == 9)) ? 1024
                  : (col && ((variant >= 3 && variant <= 5) || variant == 8)) ? 512 : 256;
   const int base = esize == 8 ? 8192 : 4096;

@@ -56,6 +56,16 @@ bool tma_col_ok(int L, const PassArgs &a);
 cudaError_t launch_tma_col_c2c_f32(int L, bool fwd, int nt, const PassArgs &a, cudaStream_t st);
 cudaError_t tma_take_fault(unsigned *fault);
 
+// Pair-column C2C kernels (fs_colpair.cu, tile variant kVariantPair): FP32
+// columns of 256, 512 or 1024 points, two neighbouring transforms per thread.
+bool colpair_length_ok(int L);
+int colpair_tile_transforms(int L);
+// Whether the 16-byte global form applies to pass `a` (complex elements):
+// unit transform distance, even point and slab strides, an even batch (no
+// pair spans two slabs), 16-byte aligned bases.
+bool colpair_vec_ok(const PassArgs &a);
+cudaError_t launch_colpair_c2c_f32(int L, bool fwd, const PassArgs &a, cudaStream_t st);
+
 // Family G: runtime-generic kernels.
 cudaError_t launch_generic(bool f64, int kind, bool col, bool fwd,
                            const GenArgs &g, cudaStream_t st);

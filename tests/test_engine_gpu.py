@@ -245,7 +245,7 @@ def test_partial_copy_coverage(prec):
 
 
 @pytest.mark.parametrize("prec", PRECS)
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 @pytest.mark.parametrize("length", [2, 8, 64, 512, 1024, 4096])
 def test_tile_variants(prec, variant, length, monkeypatch):
     """Every tile-shape candidate the planner can pick computes the same
@@ -255,6 +255,57 @@ def test_tile_variants(prec, variant, length, monkeypatch):
     for stride, dist in ((batch, 1), (1, length)):
         y, ref, h = _c2c_case(prec, length, batch, stride, dist, nv.BACKWARD, seed=variant)
         assert O.rel_l2(y, ref) < tol(prec), (variant, length, stride)
+
+
+@pytest.mark.parametrize("length,batch,stride", [
+    (512, 257, 257),    # odd point stride: 8-byte global accesses
+    (512, 258, 258),    # even stride, even batch: 16-byte global accesses
+    (512, 301, 302),    # odd batch: the last pair has one transform
+    (256, 255, 255),
+    (256, 1024, 1024),
+    (256, 96, 130),     # gaps between point rows
+])
+def test_pair_column_tile(length, batch, stride, monkeypatch):
+    """Tile variant 10 (two neighbouring transforms per thread, FP32 columns)
+    against the oracle: both directions, in place and through a fused
+    out-of-place copy."""
+    monkeypatch.setenv("B200FFT_VARIANT", "10")
+    assert "var=10" in nv.describe(nv.F32, nv.KIND_C2C, length, batch, stride, 1)
+    for direction in (nv.FORWARD, nv.BACKWARD):
+        y, ref, _ = _c2c_case(nv.F32, length, batch, stride, 1, direction, seed=stride)
+        assert O.rel_l2(y, ref) < tol(nv.F32), (length, batch, stride, direction)
+    # out of place: a held copy folded into the pass (reads src, writes dst)
+    span = (length - 1) * stride + batch
+    x = O.normal_complex(span, 3).astype(np.complex64)
+    src, dst = to_dev(x), to_dev(np.zeros_like(x))
+    h = nv.Handle(nv.F32, 1)
+    h.plan_c2c(0, length, batch, stride, 1)
+    h.memcpy(dst, src, x.nbytes)
+    h.exec_c2c(0, nv.FORWARD, dst)
+    h.sync()
+    ref = O.c2c_batch(x, length, batch, stride, 1, -1)
+    assert O.rel_l2(to_host(dst), ref) < tol(nv.F32)
+    assert np.array_equal(to_host(src), x)
+
+
+def test_pair_column_tile_across_slabs(monkeypatch):
+    """Variant 10 on a coalesced middle-axis run (the 512^3 R2C middle axis in
+    miniature: slices of [512][257], odd batch, so pairs span two slabs)."""
+    monkeypatch.setenv("B200FFT_VARIANT", "10")
+    n, nc, slabs = 512, 257, 5
+    x = O.normal_complex(slabs * n * nc, 8).astype(np.complex64)
+    d = to_dev(x)
+    h = nv.Handle(nv.F32, 2)
+    h.plan_c2c(0, n, nc, nc, 1)             # one slice
+    h.plan_c2c(1, n, slabs * nc, 1, n)      # makes the full buffer `slabs` slices
+    for i in range(slabs):
+        h.exec_c2c(0, nv.BACKWARD, int(d.data_ptr()) + i * n * nc * 8)
+    h.sync()
+    assert h.stats()["kernel_launches"] == 1
+    y = to_host(d).reshape(slabs, n * nc)
+    for i in range(slabs):
+        ref = O.c2c_batch(x[i * n * nc:(i + 1) * n * nc], n, nc, nc, 1, +1)
+        assert O.rel_l2(y[i], ref) < tol(nv.F32), i
 
 
 MIXED_STATIC = [24, 30, 40, 48, 60, 80, 96, 120, 160, 192, 384, 768]
