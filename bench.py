@@ -612,12 +612,13 @@ def measure_uneven(grids, seed, steps, warmup, gpu_index=0):
     # the dependency-scheduled form (one persistent launch over a work list of
     # (pass, tile) items), as a CUDA graph
     gs = make_group(True)
+    sched_stats = gs.stats()  # the run at group end: launches of one run
     gs.capture()
     sched_graph_ms = _timed_steps(gs.replay, steps, warmup, dflt)
-    sched_stats = gs.stats()
     gs.close()
     # the default form: per-level launches of the specialised kernels
     g = make_group(False)
+    levels_stats = g.stats()
     grouped_ms = _timed_steps(g.replay, steps, warmup, dflt)
     g.capture()
     clocks = ClockSampler(gpu_index)
@@ -654,7 +655,8 @@ def measure_uneven(grids, seed, steps, warmup, gpu_index=0):
         "loop_ms": round(loop_ms, 4), "grouped_ms": round(grouped_ms, 4),
         "graph_ms": round(graph_ms, 4), "speedup_graph_vs_loop": round(loop_ms / graph_ms, 2),
         "schedule_graph_ms": round(sched_graph_ms, 4),
-        "schedule_launches_per_run": sched_stats["kernel_launches"] // max(1, sched_stats["runs"]),
+        "schedule_launches_per_run": sched_stats["kernel_launches"],
+        "launches_per_run": levels_stats["kernel_launches"],
         "alg_bytes": alg, "hbm_frac_graph": round(alg / (graph_ms * 1e-3) / 1e9 / peak, 4),
         "peak_gbs": peak, "peak_source": peak_kind,
         "oracle": "scipy.fft FP64 per grid",

@@ -253,8 +253,9 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
       var = variant;
     if (!is_pow2(L) && !(ch.col && var == 1))
       var = 0; // mixed-radix lengths: the full tile, or the half tile for columns
-    if (var == kVariantPair &&
-        !(ch.col && kind == KIND_C2C && csize == 8 && colpair_length_ok(L)))
+    if ((var == kVariantPair &&
+         !(ch.col && kind == KIND_C2C && csize == 8 && colpair_length_ok(L))) ||
+        (var == kVariantPairWide && !(ch.col && kind == KIND_C2C && csize == 8 && L == 512)))
       var = default_variant(csize, L, ch.col, stride); // the pair tile does not apply
     const CfgS c = cfg_static(csize, L, ch.col, var);
     ch.variant = var;
@@ -420,6 +421,7 @@ struct GroupStep {
   // copy
   RecOp op;
   int level = 0; // dependency level (the level's steps are independent)
+  int chain = 0; // chain of grids the step belongs to (chains are independent)
   // SINGLE (and the first item of a STATIC step)
   b200fft_handle_s *h = nullptr;
   Plan plan;
@@ -443,12 +445,18 @@ struct b200fft_group_s {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   b200fft_stats stats{};
-  // the steps of one level run side by side: step i of a level on
-  // streams[i % size] (streams[0] is the group's stream), forked from and
-  // joined back into the group's stream by events around the level
-  std::vector<cudaStream_t> aux;
-  std::vector<cudaEvent_t> aux_done;
-  cudaEvent_t level_start = nullptr;
+  // The steps of one level run side by side: step i of a level on lane
+  // i % lanes, forked from and joined back into the chain's first lane by
+  // events around the level. Independent chains of grids
+  // (B200FFT_GROUP_CHAINS): chain c's levels run on lanes[c] (lanes[0][0] is
+  // the group's stream), forked from the group's stream at the start and
+  // joined back at the end, so one chain's level tails overlap the other
+  // chains' work.
+  int chains = 1;
+  std::vector<std::vector<cudaStream_t>> lanes;      // [chain][lane]
+  std::vector<std::vector<cudaEvent_t>> lane_done;   // [chain][lane]
+  std::vector<cudaEvent_t> chain_start;              // [chain] level fork
+  cudaEvent_t fork_ev = nullptr;
   // The dependency-scheduled form (fft_sched.cu, B200FFT_GROUP_SCHEDULE=1):
   // when every recorded pass has a tile in the schedule kernel, the whole
   // schedule is one persistent launch over a (pass, tile) work list instead
@@ -841,6 +849,8 @@ cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
         var = kVariantPair;
       if (var == kVariantPair && !f64 && p.ch.col && colpair_length_ok(p.ch.L))
         return launch_colpair_c2c_f32(p.ch.L, fwd, a, h->stream);
+      if (var == kVariantPairWide && !f64 && p.ch.col && p.ch.L == 512)
+        return launch_colpair_wide_c2c_f32(fwd, a, h->stream);
       if (var == kVariantTma || var == kVariantTma + 1) {
         if (!f64 && p.ch.col && tma_col_ok(p.ch.L, a)) {
           h->used_tma = true;
@@ -1019,7 +1029,7 @@ int autotune(H *h, Plan &p) {
   if (p.ch.family == 0) {
     if (p.ch.col) {
       const int meas[] = {0, 3, 5, 8, 10};
-      const int pat[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10};
+      const int pat[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11};
       if (rigor >= B200FFT_PLAN_PATIENT)
         for (int v : pat) cands.push_back({0, v});
       else
@@ -1665,12 +1675,19 @@ void group_free_schedule(G *g) {
     }
     if (g->d_queues)
       cudaFree(g->d_queues);
-    for (cudaStream_t s : g->aux)
-      cudaStreamDestroy(s);
-    for (cudaEvent_t e : g->aux_done)
-      cudaEventDestroy(e);
-    if (g->level_start)
-      cudaEventDestroy(g->level_start);
+    for (size_t c = 0; c < g->lanes.size(); ++c)
+      for (size_t w = 0; w < g->lanes[c].size(); ++w)
+        if (!(c == 0 && w == 0) && g->lanes[c][w])
+          cudaStreamDestroy(g->lanes[c][w]);
+    for (auto &v : g->lane_done)
+      for (cudaEvent_t e : v)
+        if (e)
+          cudaEventDestroy(e);
+    for (cudaEvent_t e : g->chain_start)
+      if (e)
+        cudaEventDestroy(e);
+    if (g->fork_ev)
+      cudaEventDestroy(g->fork_ev);
   }
   if (!g->record_only) {
     if (g->d_spasses)
@@ -1688,9 +1705,11 @@ void group_free_schedule(G *g) {
   g->d_sdone = nullptr;
   g->d_sclaim = nullptr;
   g->sbytes = 0;
-  g->aux.clear();
-  g->aux_done.clear();
-  g->level_start = nullptr;
+  g->lanes.clear();
+  g->lane_done.clear();
+  g->chain_start.clear();
+  g->fork_ev = nullptr;
+  g->chains = 1;
   g->d_queues = nullptr;
   g->nqueues = 0;
   g->steps.clear();
@@ -1878,11 +1897,42 @@ int group_build(G *g) {
   size_t depth = 0;
   for (H *h : g->handles)
     depth = std::max(depth, h->recs.size());
+  // chains: members split into groups of about equal work (largest first,
+  // each to the chain with the least so far)
+  // (default: 3 chains from 48 members on: 256 uneven grids 2.18 -> 2.12 ms,
+  // the chains' level tails overlapping; one chain below that)
+  int chains = g->handles.size() >= 48 ? 3 : 1;
+  if (const char *v = std::getenv("B200FFT_GROUP_CHAINS"))
+    chains = std::max(1, std::min(4, std::atoi(v)));
+  chains = std::max(1, std::min<int>(chains, static_cast<int>(g->handles.size())));
+  std::vector<int> chain_of(g->handles.size(), 0);
+  if (chains > 1) {
+    std::vector<std::pair<double, size_t>> work;
+    for (size_t i = 0; i < g->handles.size(); ++i) {
+      double w = 0;
+      for (const RecOp &op : g->handles[i]->recs)
+        if (op.type == RecOp::PASS)
+          w += static_cast<double>(op.plan.batch) * op.plan.len * op.slabs;
+      work.push_back({w, i});
+    }
+    std::sort(work.begin(), work.end(), [](const auto &a, const auto &b) {
+      return a.first > b.first || (a.first == b.first && a.second < b.second);
+    });
+    std::vector<double> load(static_cast<size_t>(chains), 0.0);
+    for (const auto &wi : work) {
+      const size_t c = static_cast<size_t>(std::min_element(load.begin(), load.end()) - load.begin());
+      chain_of[wi.second] = static_cast<int>(c);
+      load[c] += wi.first;
+    }
+  }
+  g->chains = chains;
+  for (int chain = 0; chain < chains; ++chain)
   for (size_t d = 0; d < depth; ++d) {
     const size_t first_step = g->steps.size();
     std::map<long long, size_t> bucket; // (static, L, f64, kind, col, fwd) -> step index
-    for (H *h : g->handles) {
-      if (d >= h->recs.size())
+    for (size_t hix = 0; hix < g->handles.size(); ++hix) {
+      H *h = g->handles[hix];
+      if (chain_of[hix] != chain || d >= h->recs.size())
         continue;
       const RecOp &op = h->recs[d];
       if (op.type != RecOp::PASS) {
@@ -1968,34 +2018,48 @@ int group_build(G *g) {
     }
     for (size_t i = first_step; i < g->steps.size(); ++i) {
       g->steps[i].level = static_cast<int>(d);
+      g->steps[i].chain = chain;
       if (g->steps[i].type == GroupStep::STATIC && g->steps[i].sitems.size() == 1)
         g->steps[i].type = GroupStep::SINGLE;
     }
   }
-  // streams for the widest level (at most kGroupStreams side by side)
+  // lanes (streams) of each chain: as many as its widest level, at most
+  // kGroupStreams over all chains; lane 0 of chain 0 is the group's stream
   if (!g->record_only) {
-    size_t widest = 1, run = 0;
+    std::vector<size_t> widest(static_cast<size_t>(chains), 1);
+    size_t run = 0;
     for (size_t i = 0; i < g->steps.size(); ++i) {
-      run = (i > 0 && g->steps[i].level == g->steps[i - 1].level) ? run + 1 : 1;
-      widest = std::max(widest, run);
+      const bool same = i > 0 && g->steps[i].level == g->steps[i - 1].level &&
+                        g->steps[i].chain == g->steps[i - 1].chain;
+      run = same ? run + 1 : 1;
+      size_t &w = widest[static_cast<size_t>(g->steps[i].chain)];
+      w = std::max(w, run);
     }
-    const size_t naux = std::min(widest, static_cast<size_t>(kGroupStreams)) - 1;
-    if (naux > 0) {
-      cudaError_t e = cudaEventCreateWithFlags(&g->level_start, cudaEventDisableTiming);
-      for (size_t k = 0; k < naux && e == cudaSuccess; ++k) {
-        cudaStream_t s = nullptr;
-        e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    const size_t per_chain = std::max<size_t>(1, kGroupStreams / static_cast<size_t>(chains));
+    cudaError_t e = cudaSuccess;
+    if (chains > 1)
+      e = cudaEventCreateWithFlags(&g->fork_ev, cudaEventDisableTiming);
+    g->lanes.resize(static_cast<size_t>(chains));
+    g->lane_done.resize(static_cast<size_t>(chains));
+    g->chain_start.assign(static_cast<size_t>(chains), nullptr);
+    for (int c = 0; c < chains && e == cudaSuccess; ++c) {
+      const size_t nl = std::min(widest[static_cast<size_t>(c)], per_chain);
+      e = cudaEventCreateWithFlags(&g->chain_start[static_cast<size_t>(c)], cudaEventDisableTiming);
+      for (size_t w = 0; w < nl && e == cudaSuccess; ++w) {
+        cudaStream_t st = g->stream;
+        if (!(c == 0 && w == 0))
+          e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
         if (e == cudaSuccess)
-          g->aux.push_back(s);
+          g->lanes[static_cast<size_t>(c)].push_back(st);
         cudaEvent_t ev = nullptr;
         if (e == cudaSuccess)
           e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
         if (e == cudaSuccess)
-          g->aux_done.push_back(ev);
+          g->lane_done[static_cast<size_t>(c)].push_back(ev);
       }
-      if (e != cudaSuccess)
-        return cuda_fail(e, "group streams");
     }
+    if (e != cudaSuccess)
+      return cuda_fail(e, "group streams");
   }
   // device copies of the work lists, one queue counter per grouped launch
   int q = 0;
@@ -2095,23 +2159,33 @@ int group_run(G *g) {
   if (g->record_only)
     return B200FFT_SUCCESS;
   cudaGetLastError(); // report only errors of the calls below
-  const size_t nstreams = 1 + g->aux.size();
+  if (g->chains > 1) { // fork: every chain starts after the work before the group
+    cudaError_t e = cudaEventRecord(g->fork_ev, g->stream);
+    for (int c = 1; c < g->chains && e == cudaSuccess; ++c)
+      e = cudaStreamWaitEvent(g->lanes[static_cast<size_t>(c)][0], g->fork_ev, 0);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "group chain fork");
+  }
   for (size_t lv = 0; lv < g->steps.size();) {
     size_t lv_end = lv;
-    while (lv_end < g->steps.size() && g->steps[lv_end].level == g->steps[lv].level)
+    while (lv_end < g->steps.size() && g->steps[lv_end].level == g->steps[lv].level &&
+           g->steps[lv_end].chain == g->steps[lv].chain)
       ++lv_end;
+    const size_t ch = static_cast<size_t>(g->steps[lv].chain);
+    const std::vector<cudaStream_t> &lanes = g->lanes[ch];
+    const size_t nstreams = lanes.size();
+    cudaStream_t main_st = lanes[0];
     const size_t width = std::min(lv_end - lv, nstreams);
-    if (width > 1) { // fork: the level's other streams start after the previous level
-      cudaError_t e = cudaEventRecord(g->level_start, g->stream);
+    if (width > 1) { // fork: the level's other lanes start after the previous level
+      cudaError_t e = cudaEventRecord(g->chain_start[ch], main_st);
       for (size_t k = 1; k < width && e == cudaSuccess; ++k)
-        e = cudaStreamWaitEvent(g->aux[k - 1], g->level_start, 0);
+        e = cudaStreamWaitEvent(lanes[k], g->chain_start[ch], 0);
       if (e != cudaSuccess)
         return cuda_fail(e, "group level fork");
     }
     for (size_t i = lv; i < lv_end; ++i) {
       GroupStep &s = g->steps[i];
-      const size_t lane = (i - lv) % nstreams;
-      cudaStream_t st = lane == 0 ? g->stream : g->aux[lane - 1];
+      cudaStream_t st = lanes[(i - lv) % nstreams];
       cudaError_t e = cudaSuccess;
       const char *what = "grouped pass";
       if (s.type == GroupStep::PASSES) {
@@ -2158,17 +2232,28 @@ int group_run(G *g) {
         return cuda_fail(e, buf);
       }
     }
-    if (width > 1) { // join: the next level starts after all of this one
+    if (width > 1) { // join: the chain's next level starts after all of this one
       cudaError_t e = cudaSuccess;
       for (size_t k = 1; k < width && e == cudaSuccess; ++k) {
-        e = cudaEventRecord(g->aux_done[k - 1], g->aux[k - 1]);
+        e = cudaEventRecord(g->lane_done[ch][k], lanes[k]);
         if (e == cudaSuccess)
-          e = cudaStreamWaitEvent(g->stream, g->aux_done[k - 1], 0);
+          e = cudaStreamWaitEvent(main_st, g->lane_done[ch][k], 0);
       }
       if (e != cudaSuccess)
         return cuda_fail(e, "group level join");
     }
     lv = lv_end;
+  }
+  if (g->chains > 1) { // join: the group's stream waits for every chain
+    cudaError_t e = cudaSuccess;
+    for (int c = 1; c < g->chains && e == cudaSuccess; ++c) {
+      e = cudaEventRecord(g->lane_done[static_cast<size_t>(c)][0],
+                          g->lanes[static_cast<size_t>(c)][0]);
+      if (e == cudaSuccess)
+        e = cudaStreamWaitEvent(g->stream, g->lane_done[static_cast<size_t>(c)][0], 0);
+    }
+    if (e != cudaSuccess)
+      return cuda_fail(e, "group chain join");
   }
   return B200FFT_SUCCESS;
 }

@@ -207,17 +207,20 @@ print(st["kernel_launches"], st["copies_issued"])
 
 
 @pytest.mark.skipif(not _drivers_built(), reason="ParaFaFT drivers not built")
-@pytest.mark.parametrize("form", ["schedule", "levels"])
+@pytest.mark.parametrize("form", ["schedule", "levels", "chains"])
 def test_group_schedules_many_grids_per_depth_and_length(form, monkeypatch):
     """256 ParaFaFT_R2C<3> objects of uneven sizes, forward+backward recorded in
-    one group, 256*6 passes, no copies. Default: at each of the 6 pass depths
-    one grouped launch per distinct kernel length (every side here has a
-    specialised kernel). With B200FFT_GROUP_SCHEDULE=1: the dependency-
-    scheduled form, one persistent launch for the whole schedule."""
+    one group, 256*6 passes, no copies. One chain (B200FFT_GROUP_CHAINS=1): at
+    each of the 6 pass depths one grouped launch per distinct kernel length
+    (every side here has a specialised kernel). Default (256 members: three
+    chains of grids): the same per chain. B200FFT_GROUP_SCHEDULE=1: the
+    dependency-scheduled form, one persistent launch for the whole schedule."""
+    monkeypatch.delenv("B200FFT_GROUP_SCHEDULE", raising=False)
+    monkeypatch.delenv("B200FFT_GROUP_CHAINS", raising=False)
     if form == "schedule":
         monkeypatch.setenv("B200FFT_GROUP_SCHEDULE", "1")
-    else:
-        monkeypatch.delenv("B200FFT_GROUP_SCHEDULE", raising=False)
+    elif form == "levels":
+        monkeypatch.setenv("B200FFT_GROUP_CHAINS", "1")
     out = _run_record(r'''
 import ctypes as C, numpy as np
 from parafaft_b200 import native as nv
@@ -244,6 +247,8 @@ print(st["kernel_launches"], st["passes_per_run"], st["copies_issued"], expect)
     assert passes == str(256 * 6) and copies == "0"
     if form == "levels":
         assert launches == expect and int(launches) <= 6 * 9
+    elif form == "chains":
+        assert int(expect) < int(launches) <= 3 * int(expect)
     else:
         assert launches == "1"
 
