@@ -253,9 +253,8 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
       var = variant;
     if (!is_pow2(L) && !(ch.col && var == 1))
       var = 0; // mixed-radix lengths: the full tile, or the half tile for columns
-    if ((var == kVariantPair &&
-         !(ch.col && kind == KIND_C2C && csize == 8 && colpair_length_ok(L))) ||
-        (var == kVariantPairWide && !(ch.col && kind == KIND_C2C && csize == 8 && L == 512)))
+    if (var == kVariantPair &&
+        !(ch.col && kind == KIND_C2C && csize == 8 && colpair_length_ok(L)))
       var = default_variant(csize, L, ch.col, stride); // the pair tile does not apply
     const CfgS c = cfg_static(csize, L, ch.col, var);
     ch.variant = var;
@@ -849,8 +848,6 @@ cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
         var = kVariantPair;
       if (var == kVariantPair && !f64 && p.ch.col && colpair_length_ok(p.ch.L))
         return launch_colpair_c2c_f32(p.ch.L, fwd, a, h->stream);
-      if (var == kVariantPairWide && !f64 && p.ch.col && p.ch.L == 512)
-        return launch_colpair_wide_c2c_f32(fwd, a, h->stream);
       if (var == kVariantTma || var == kVariantTma + 1) {
         if (!f64 && p.ch.col && tma_col_ok(p.ch.L, a)) {
           h->used_tma = true;
@@ -1029,7 +1026,7 @@ int autotune(H *h, Plan &p) {
   if (p.ch.family == 0) {
     if (p.ch.col) {
       const int meas[] = {0, 3, 5, 8, 10};
-      const int pat[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11};
+      const int pat[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10};
       if (rigor >= B200FFT_PLAN_PATIENT)
         for (int v : pat) cands.push_back({0, v});
       else

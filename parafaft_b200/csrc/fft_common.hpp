@@ -366,14 +366,11 @@ struct CfgS {
 //  10 = pair-column tile (FP32, 256/512/1024 points): 512 (1024) threads, two
 //       neighbouring transforms per thread, 16-byte shared-memory exchanges
 //       and twiddles shared by the pair (fft_colpair.cuh).
-//  11 = wide pair-column tile (FP32, 512 points): 1024 threads, 32
-//       transforms (16 pairs, 256-byte row segments), one CTA per SM.
 // Where a TMA or pair variant does not apply, the plan's default tile runs
 // instead.
-constexpr int kStaticVariants = 12;
+constexpr int kStaticVariants = 11;
 constexpr int kVariantTma = 8;
 constexpr int kVariantPair = 10;
-constexpr int kVariantPairWide = 11;
 constexpr int kVariantStaged = 4;
 constexpr int kVariantPipelined = 6;
 
@@ -407,9 +404,7 @@ constexpr CfgS cfg_static(int esize, int L, bool col, int variant = 0) {
     const int nt = L == 1024 ? 1024 : 512;
     return CfgS{nt, TB, nt / (TB / 2), L / (nt / (TB / 2))};
   }
-  if (col && variant == 11 && esize == 8 && L == 512)
-    return CfgS{1024, 32, 64, 8};
-  if (variant == 10 || variant == 11)
+  if (variant == 10)
     variant = 5; // the pair tile's shape where it does not apply
   const int NT = (col && (variant == 7 || variant == 9)) ? 1024
                  : (col && ((variant >= 3 && variant <= 5) || variant == 8)) ? 512 : 256;

@@ -66,8 +66,4 @@ cudaError_t launch_colpair_c2c_f32(int L, bool fwd, const PassArgs &a, cudaStrea
   }
 }
 
-cudaError_t launch_colpair_wide_c2c_f32(bool fwd, const PassArgs &a, cudaStream_t st) {
-  return launch_colpair_l<512, 1024, 32>(fwd, a, st); // 16 pairs, 256-byte rows
-}
-
 } // namespace b200fft

@@ -65,9 +65,6 @@ int colpair_tile_transforms(int L);
 // pair spans two slabs), 16-byte aligned bases.
 bool colpair_vec_ok(const PassArgs &a);
 cudaError_t launch_colpair_c2c_f32(int L, bool fwd, const PassArgs &a, cudaStream_t st);
-// The wide form for 512 points (tile variant kVariantPairWide): 1024 threads,
-// 32 transforms per tile, one CTA per SM.
-cudaError_t launch_colpair_wide_c2c_f32(bool fwd, const PassArgs &a, cudaStream_t st);
 
 // Family G: runtime-generic kernels.
 cudaError_t launch_generic(bool f64, int kind, bool col, bool fwd,
