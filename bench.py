@@ -44,9 +44,9 @@ ALG_BYTES = 6463422464  # one read + one write per fused pass, fwd+bwd
 
 # DRAM bytes (read + write) per launch from the last `ncu --set full` capture
 # of the same kernels (profiles/r2c512_kernels_ncu_full.md).
-NCU_TRAFFIC = {"r2c_fwd": 1021216000, "c2c_stage1_fwd": 1031302144,
-               "c2c_stage2_fwd": 1029826304, "c2c_stage2_bwd": 1024527616,
-               "c2c_stage1_bwd": 1032372992, "c2r_bwd": 1036700160}
+NCU_TRAFFIC = {"r2c_fwd": 1020436736, "c2c_stage1_fwd": 1030280192,
+               "c2c_stage2_fwd": 1028872448, "c2c_stage2_bwd": 1020416000,
+               "c2c_stage1_bwd": 1034022144, "c2r_bwd": 1037415424}
 
 
 def _peaks():
