@@ -55,8 +55,6 @@ bool colpair_vec_ok(const PassArgs &a) {
 
 bool colpair_length_ok(int L) { return L == 256 || L == 512 || L == 1024; }
 
-int colpair_tile_transforms(int L) { return L == 256 ? 32 : (L == 512 || L == 1024) ? 16 : 0; }
-
 cudaError_t launch_colpair_c2c_f32(int L, bool fwd, const PassArgs &a, cudaStream_t st) {
   switch (L) {
   case 256: return launch_colpair_l<256, 512, 32>(fwd, a, st); // 8 points per thread, 256-byte rows

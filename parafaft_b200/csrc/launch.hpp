@@ -59,7 +59,6 @@ cudaError_t tma_take_fault(unsigned *fault);
 // Pair-column C2C kernels (fs_colpair.cu, tile variant kVariantPair): FP32
 // columns of 256, 512 or 1024 points, two neighbouring transforms per thread.
 bool colpair_length_ok(int L);
-int colpair_tile_transforms(int L);
 // Whether the 16-byte global form applies to pass `a` (complex elements):
 // unit transform distance, even point and slab strides, an even batch (no
 // pair spans two slabs), 16-byte aligned bases.
@@ -103,7 +102,6 @@ struct SchedArgs {
 // when the schedule kernel does not carry it; transforms per tile of a spec.
 int sched_spec_index(int kind, bool col, bool fwd, int L);
 int sched_tile_transforms(int spec);
-size_t sched_smem_bytes();
 // CTAs of a persistent launch on the current device (all resident at once).
 cudaError_t sched_grid(int *grid);
 cudaError_t launch_sched(const SchedArgs &s, int grid, cudaStream_t st);
