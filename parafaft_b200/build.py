@@ -39,7 +39,8 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC"] + ARCH
 
 ENGINE_SOURCES = ["api.cu", "fg.cu", "fs_c2c_f32.cu", "fs_c2c_f64.cu",
                   "fs_r2c_f32.cu", "fs_r2c_f64.cu", "fft_tc.cu", "fft_tc5.cu", "fft_tma.cu",
-                  "noalloc.cu", "fft_sched.cu", "fs_colpair.cu"]
+                  "noalloc.cu", "fft_sched.cu", "fs_colpair.cu",
+                  "fft_tc5col.cu"]
 
 
 def _nvcc() -> str:

@@ -235,6 +235,15 @@ int choose_kernel(int prec, int kind, int len, long long batch, long long stride
       ch.TB = 8;
       ch.NT = 128;
     }
+    // 512-point columns: the mma.sync kernel by default; B200FFT_TC_FORM=tc5
+    // runs them on the tcgen05 column kernel (family 5: correct, but its
+    // tiles are not pipelined and it ran 0.44-0.49 ms against 0.31-0.43 ms
+    // for the mma.sync form on the 512^3 column passes)
+    if (ch.col && L == 512 && form != nullptr && std::string(form) == "tc5") {
+      ch.family = 5;
+      ch.TB = 16;
+      ch.NT = 512;
+    }
     *out = ch;
     return B200FFT_SUCCESS;
   }
@@ -332,6 +341,7 @@ std::string describe_choice(const Choice &ch, int kind) {
                 ch.family == 0   ? "static"
                 : ch.family == 2 ? "split-tc"
                 : ch.family == 3 ? "split-tc5"
+                : ch.family == 5 ? "split-tc5col"
                                  : "generic",
                 kn, ch.L,
                 ch.col ? "col" : "row", ch.TB, ch.NT, rad.c_str(), ch.variant);
@@ -871,6 +881,9 @@ cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
   } else if (p.ch.family == 3) {
     h->used_tc5 = true;
     e = launch_tc5_row256_f32(fwd, a, h->stream);
+  } else if (p.ch.family == 5) {
+    h->used_tc5 = true;
+    e = launch_tc5_col512_f32(fwd, a, h->stream);
   } else {
     GenArgs g = p.ch.gen;
     g.p = a;
@@ -1443,10 +1456,13 @@ int b200fft_sync(b200fft_handle h) {
                   "(results of that launch are invalid)");
   }
   if (h->used_tc5) {
-    unsigned fault = 0;
+    unsigned fault = 0, fault_col = 0;
     e = tc5_take_fault(&fault);
+    if (e == cudaSuccess)
+      e = tc5col_take_fault(&fault_col);
     if (e != cudaSuccess)
       return cuda_fail(e, "tensor-core fault word");
+    fault |= fault_col;
     if (fault)
       return fail(B200FFT_ERR_DEVICE_STATUS,
                   "b200fft: a tensor-core kernel gave up waiting for its products "

@@ -46,9 +46,12 @@ constexpr bool tc_length_ok(int L) { return L == 256 || L == 512 || L == 1024; }
 // The same on the fifth-generation tensor cores (tcgen05, TMEM accumulators):
 // FP32 C2C rows of length 256.
 cudaError_t launch_tc5_row256_f32(bool fwd, const PassArgs &a, cudaStream_t st);
-// The tcgen05 kernels' device fault word (a bounded wait that ran out),
+// FP32 C2C columns of length 512 on tcgen05 (fft_tc5col.cu).
+cudaError_t launch_tc5_col512_f32(bool fwd, const PassArgs &a, cudaStream_t st);
+// The tcgen05 kernels' device fault words (a bounded wait that ran out),
 // returned and cleared; call after the launches' stream is synchronised.
 cudaError_t tc5_take_fault(unsigned *fault);
+cudaError_t tc5col_take_fault(unsigned *fault);
 // TMA-fed FP32 column C2C passes (fft_tma.cu): eligibility (lengths 256, 512,
 // 1024; contiguous transforms; 16-byte aligned base, stride and slab
 // stride), the launch (nt = 512 or 1024 threads per CTA) and the fault word.

@@ -188,16 +188,23 @@ def test_rows_256_mma_sync_form(direction, monkeypatch):
     assert O.rel_l2(y, ref) < REL_F32
 
 
-def test_tcgen05_wait_limit_reports_device_status(monkeypatch):
-    """The tcgen05 kernel bounds every wait for its products. With the test
-    switch set, thread 0 issues nothing and waits on a barrier phase that never
-    completes: the wait runs out (about a second), the CTAs free their tensor
-    memory and return, and b200fft_sync reports B200FFT_ERR_DEVICE_STATUS. The
-    context stays usable: the next transform is correct."""
-    x = O.normal_complex(256 * 16, 4)
+@pytest.mark.parametrize("length,col,prefix", [(256, False, "split-tc5 "),
+                                               (512, True, "split-tc5col")])
+def test_tcgen05_wait_limit_reports_device_status(monkeypatch, length, col, prefix):
+    """The tcgen05 kernels (256-point rows, 512-point columns) bound every wait
+    for their products. With the test switch set, thread 0 issues nothing and
+    waits on a barrier phase that never completes: the wait runs out (about a
+    second), the CTAs free their tensor memory and return, and b200fft_sync
+    reports B200FFT_ERR_DEVICE_STATUS. The context stays usable: the next
+    transform is correct."""
+    batch = 16
+    stride, dist = (batch, 1) if col else (1, length)
+    x = O.normal_complex(length * batch, 4)
+    if col:  # the tcgen05 column kernel is chosen with B200FFT_TC_FORM=tc5
+        monkeypatch.setenv("B200FFT_TC_FORM", "tc5")
     h = nv.Handle(nv.F32, 1, flags=nv.FLAG_SPLIT_TC)
-    h.plan_c2c(0, 256, 16, 1, 256)
-    assert h.plan_describe(nv.KIND_C2C, 0).startswith("split-tc5")
+    h.plan_c2c(0, length, batch, stride, dist)
+    assert h.plan_describe(nv.KIND_C2C, 0).startswith(prefix)
     d = to_dev(x.astype(np.complex64))
     monkeypatch.setenv("B200FFT_TC5_STALL_TEST", "1")
     h.exec_c2c(0, nv.FORWARD, d)
@@ -208,5 +215,27 @@ def test_tcgen05_wait_limit_reports_device_status(monkeypatch):
     d = to_dev(x.astype(np.complex64))
     h.exec_c2c(0, nv.FORWARD, d)
     h.sync()
-    ref = O.c2c_batch(x, 256, 16, 1, 256, -1)
+    ref = O.c2c_batch(x, length, batch, stride, dist, -1)
     assert O.rel_l2(to_host(d), ref) < REL_F32
+
+
+@pytest.mark.parametrize("direction", [nv.FORWARD, nv.BACKWARD])
+@pytest.mark.parametrize("batch,slabs", [(45, None), (21, 5), (32, 3)])
+def test_columns_512_tcgen05_form(direction, batch, slabs, monkeypatch):
+    """512-point columns on the tcgen05 column kernel (B200FFT_TC_FORM=tc5):
+    partial tiles, coalesced middle-axis slabs with tiles straddling slab
+    boundaries, both directions; within 2e-6 and twice the plain error."""
+    monkeypatch.setenv("B200FFT_TC_FORM", "tc5")
+    if slabs is None:
+        x = O.normal_complex(512 * batch, 6)
+        e_tc, _ = _check(x, 512, batch, batch, 1, direction)
+    else:
+        x = O.normal_complex(slabs * 512 * batch, 9)
+        sign = -1 if direction == nv.FORWARD else +1
+        ref = (np.fft.fft if sign < 0 else lambda v, axis: np.fft.ifft(v, axis=axis) * 512)(
+            x.reshape(slabs, 512, batch), axis=1).ravel()
+        e_tc, _ = _check(x, 512, batch, batch, 1, direction, slabs=(slabs, 512 * batch),
+                         span_ref=ref)
+    _, desc = _run(x, 512, batch, batch, 1, direction, True,
+                   None if slabs is None else (slabs, 512 * batch))
+    assert desc.startswith("split-tc5col c2c L=512 col"), desc
