@@ -2140,6 +2140,9 @@ int group_run(G *g) {
     g->stats.bytes_transformed += static_cast<uint64_t>(g->sbytes);
     if (g->record_only)
       return B200FFT_SUCCESS;
+    if (g->d_sdone == nullptr || g->d_spasses == nullptr || g->d_sorder == nullptr)
+      return fail(B200FFT_ERR_INVALID_ARG,
+                  "b200fft: the group's schedule was not built (b200fft_group_end failed)");
     cudaGetLastError();
     // zero the pass counters and the claim word (not the fault word)
     const size_t claim_end = reinterpret_cast<char *>(g->d_sclaim + 1) -
