@@ -40,6 +40,9 @@ SHAPE = (512, 512, 512)
 SEED = 1234
 METRIC = "512^3 FP32 R2C fwd+bwd ms, % HBM roofline; plain vs split-TC at rel-L2<=2e-6"
 WORKLOAD = "ParaFaFT_R2C<3, float> 512x512x512 forward_in_place+backward_in_place"
+# the `config` of both arms' lines (the same workload, named the same way)
+CONFIG = {"workload": WORKLOAD, "shape": list(SHAPE),
+          "l2": "inputs larger than L2 (539 MB buffer)"}
 ALG_BYTES = 6463422464  # one read + one write per fused pass, fwd+bwd
 
 # DRAM bytes (read + write) per launch from the last `ncu --set full` capture
@@ -196,7 +199,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": n, "warmup": min(args.warmup, 1),
         "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1), seed 1234",
-        "config": {"workload": WORKLOAD, "l2": "host path"},
+        "config": dict(CONFIG), "method": "scipy.fft float32 on the host cores",
         "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": cores, "kind": "port",
                          "sample": f"{n} full 512^3 fwd+bwd steps, scipy.fft float32 "
                                    f"(FFTWBackend<float> stand-in: libfftw3f absent)"},
@@ -952,9 +955,7 @@ def run_b200(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic N(0,1) float32, seed 1234",
-            "config": {"workload": WORKLOAD, "shape": list(SHAPE), "method": "plain FP32 Stockham",
-                       "l2": "inputs larger than L2 (539 MB buffer)",
-                       "replicas": world},
+            "config": dict(CONFIG), "method": "plain FP32 Stockham", "replicas": world,
             "rel_l2_fwd_vs_fp64": rel_fwd, "rel_l2_roundtrip": rel_rt,
             "step_ms_median": round(statistics.median(per_step), 4),
             "step_ms_mean_per_step_events": round(statistics.fmean(per_step), 4),

@@ -27,6 +27,11 @@ def test_reference_arm_prints_the_contract_line():
     assert d["higher_is_better"] is False and d["n_gpus"] == 1
     assert d["steps"] == 1 and d["warmup"] == 1
     assert isinstance(d["config"], dict) and "workload" in d["config"]
+    # the same config object as the B200 arm's line (same workload, same keys)
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert d["config"] == bench.CONFIG
+    assert d["metric"] == bench.METRIC
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["unit"] == d["unit"]
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["sample"]
