@@ -81,14 +81,15 @@ def test_no_alloc_rejects_lengths_beyond_its_array():
 
 
 def test_no_alloc_leaves_device_memory_unchanged():
-    """After a first call on the device (which may load the kernels), further
-    calls change neither the device's free memory nor PyTorch's allocations:
-    the entry point allocates nothing."""
+    """After first calls on the device (which may load the kernels they
+    launch), further calls change neither the device's free memory nor
+    PyTorch's allocations: the entry point allocates nothing."""
     import torch
     prec, length, batch = nv.F32, 1024, 64
     x = to_dev(O.normal_complex(length * batch, 12).astype(np.complex64))
     out = torch.empty_like(x)
-    nv.c2c_noalloc(prec, nv.FORWARD, length, batch, 1, length, x, out)
+    for direction in (nv.FORWARD, nv.BACKWARD):
+        nv.c2c_noalloc(prec, direction, length, batch, 1, length, x, out)
     torch.cuda.synchronize()
     free0 = torch.cuda.mem_get_info()[0]
     reserved0 = torch.cuda.memory_reserved()
