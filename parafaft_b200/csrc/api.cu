@@ -1738,15 +1738,66 @@ int sm_count_current() {
   return n;
 }
 
-// Elements (complex) a pass spans on one side, from its first element to its
-// last: the last point of the last transform of the last slab.
-long long pass_extent(const PassArgs &a, int points, bool in) {
-  const long long slabs = a.batch > 0 ? (a.total + a.batch - 1) / a.batch : 1;
-  const long long dist = in ? a.idist : a.odist;
-  const long long stride = in ? a.istride : a.ostride;
-  const long long slab = in ? a.islab : a.oslab;
-  return (slabs - 1) * slab + (std::min(a.total, a.batch) - 1) * dist +
-         static_cast<long long>(points - 1) * stride + 1;
+// Whether no two members of the group touch the same memory in their
+// recorded operations (each member's passes and copies as byte intervals,
+// over-approximated per pass by its padded extent). Forms of the schedule
+// that run one member's later passes beside another member's earlier ones
+// (chains, the dependency-scheduled kernel) need it; the level barriers of
+// one chain do not.
+bool members_disjoint(const G *g) {
+  struct Span {
+    uintptr_t lo, hi;
+  };
+  std::vector<Span> spans; // every member's memory, as disjoint intervals
+  for (const H *h : g->handles) {
+    std::vector<Span> own;
+    const size_t cs = h->csize(), rs = static_cast<size_t>(h->rsize);
+    auto add = [&](const void *p, size_t bytes) {
+      const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+      own.push_back({a, a + bytes});
+    };
+    for (const RecOp &op : h->recs) {
+      if (op.type == RecOp::COPY) {
+        add(op.dst, op.bytes);
+        add(op.src, op.bytes);
+      } else if (op.type == RecOp::COPY2D) {
+        add(op.dst, op.dpitch * (op.height - 1) + op.width);
+        add(op.src, op.spitch * (op.height - 1) + op.width);
+      } else {
+        const Plan &p = op.plan;
+        size_t bytes;
+        if (p.kind == KIND_C2C) {
+          const long long span = static_cast<long long>(p.len - 1) * p.stride +
+                                 (p.batch - 1) * p.dist + 1;
+          bytes = static_cast<size_t>((op.slabs - 1) * op.slab + span) * cs;
+        } else { // padded real rows, dist in reals
+          bytes = static_cast<size_t>((p.batch - 1) * p.dist +
+                                      2ll * (p.len / 2 + 1) * p.stride) * rs;
+        }
+        add(op.in, bytes);
+        add(op.out, bytes);
+      }
+    }
+    // union of this member's intervals (its operations share its buffers)
+    std::sort(own.begin(), own.end(), [](const Span &a, const Span &b) { return a.lo < b.lo; });
+    const size_t first = spans.size();
+    for (const Span &x : own) {
+      if (spans.size() > first && x.lo <= spans.back().hi)
+        spans.back().hi = std::max(spans.back().hi, x.hi);
+      else
+        spans.push_back(x);
+    }
+  }
+  // sorted by start, each interval begins at or after the furthest end before
+  // it (a member's own intervals are disjoint after the union)
+  std::sort(spans.begin(), spans.end(), [](const Span &a, const Span &b) { return a.lo < b.lo; });
+  uintptr_t reach = 0;
+  for (const Span &x : spans) {
+    if (x.lo < reach)
+      return false;
+    reach = std::max(reach, x.hi);
+  }
+  return true;
 }
 
 // The dependency-scheduled form of a group (fft_sched.cu), chosen with
@@ -1762,10 +1813,8 @@ bool sched_build(G *g, int *rc) {
   *rc = B200FFT_SUCCESS;
   if (!env_flag("B200FFT_GROUP_SCHEDULE"))
     return false;
-  struct Span {
-    uintptr_t lo, hi;
-  };
-  std::vector<Span> spans; // every member's memory, as disjoint intervals
+  if (!members_disjoint(g))
+    return false; // members share memory: keep the level barriers
   std::vector<SchedPass> passes;
   std::vector<std::pair<long long, int>> keyed; // (order key, pass)
   // a pass is listed `lag` keys after its dependency; lag >= 1 keeps every
@@ -1779,7 +1828,6 @@ bool sched_build(G *g, int *rc) {
     H *h = g->handles[hi];
     if (h->prec != B200FFT_F32 || h->recs.empty())
       return false;
-    std::vector<Span> own; // this member's pass sides
     int prev = -1;
     for (size_t k = 0; k < h->recs.size(); ++k) {
       const RecOp &op = h->recs[k];
@@ -1805,40 +1853,11 @@ bool sched_build(G *g, int *rc) {
       q.ntiles = static_cast<unsigned>(nt);
       q.dep = prev;
       q.need = prev >= 0 ? passes[static_cast<size_t>(prev)].ntiles : 0;
-      const size_t cs = h->csize();
-      const uintptr_t in0 = reinterpret_cast<uintptr_t>(q.a.in);
-      const uintptr_t out0 = reinterpret_cast<uintptr_t>(q.a.out);
-      // points per transform on each side: R2C rows read L complex (2L reals)
-      // and write L+1, C2R rows the reverse
-      const int pin = p.kind == KIND_C2R ? sc.L + 1 : sc.L;
-      const int pout = p.kind == KIND_R2C ? sc.L + 1 : sc.L;
-      const uintptr_t in1 = in0 + cs * static_cast<uintptr_t>(pass_extent(q.a, pin, true));
-      const uintptr_t out1 = out0 + cs * static_cast<uintptr_t>(pass_extent(q.a, pout, false));
-      own.push_back({in0, in1});
-      own.push_back({out0, out1});
       bytes += pass_bytes(h, p, q.a.total);
       prev = static_cast<int>(passes.size());
       keyed.push_back({static_cast<long long>(hi) + lag * static_cast<long long>(k), prev});
       passes.push_back(q);
     }
-    // union of this member's intervals (its passes share its buffers)
-    std::sort(own.begin(), own.end(), [](const Span &a, const Span &b) { return a.lo < b.lo; });
-    const size_t first = spans.size();
-    for (const Span &x : own) {
-      if (spans.size() > first && x.lo <= spans.back().hi)
-        spans.back().hi = std::max(spans.back().hi, x.hi);
-      else
-        spans.push_back(x);
-    }
-  }
-  // members' intervals must not meet: sorted by start, each begins at or
-  // after the furthest end before it (a member's own intervals are disjoint)
-  std::sort(spans.begin(), spans.end(), [](const Span &a, const Span &b) { return a.lo < b.lo; });
-  uintptr_t reach = 0;
-  for (const Span &x : spans) {
-    if (x.lo < reach)
-      return false; // members share memory: keep the level barriers
-    reach = std::max(reach, x.hi);
   }
   // list order: by key; within a key, later passes (of grids further ahead)
   // first, their dependencies being the oldest
@@ -1918,6 +1937,8 @@ int group_build(G *g) {
   if (const char *v = std::getenv("B200FFT_GROUP_CHAINS"))
     chains = std::max(1, std::min(4, std::atoi(v)));
   chains = std::max(1, std::min<int>(chains, static_cast<int>(g->handles.size())));
+  if (chains > 1 && !members_disjoint(g))
+    chains = 1; // members share memory: one chain, every level a barrier
   std::vector<int> chain_of(g->handles.size(), 0);
   if (chains > 1) {
     std::vector<std::pair<double, size_t>> work;

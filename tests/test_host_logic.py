@@ -256,9 +256,11 @@ print(st["kernel_launches"], st["passes_per_run"], st["copies_issued"], expect)
 @pytest.mark.skipif(not _drivers_built(), reason="ParaFaFT drivers not built")
 def test_group_members_sharing_memory_keep_level_barriers(monkeypatch):
     """Two grids transformed in the same buffer are not independent: the
-    group keeps its per-level launches even when the dependency schedule is
-    asked for (it orders only each grid's own passes)."""
+    group keeps one chain of per-level launches even when the dependency
+    schedule or several chains are asked for (both order only each grid's
+    own passes): three levels, one launch each for the two equal grids."""
     monkeypatch.setenv("B200FFT_GROUP_SCHEDULE", "1")
+    monkeypatch.setenv("B200FFT_GROUP_CHAINS", "2")
     out = _run_record(r'''
 import ctypes as C
 from parafaft_b200 import native as nv
@@ -272,7 +274,7 @@ b.forward(buf.value)
 g.end()
 print(g.stats()["kernel_launches"])
 ''')
-    assert int(out.split()[0]) > 1
+    assert int(out.split()[0]) == 3
 
 
 def test_wisdom_roundtrip_and_plan_choice(tmp_path):
