@@ -852,7 +852,8 @@ cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
       // on 16-byte aligned rows (the first axis of a grid) take the pair tile
       // by default: 16-byte loads, stores and exchanges (512^3 first-axis
       // pass 0.212 -> 0.195 ms); odd point strides keep the one-transform
-      // tile (the pair tile's 8-byte form was slower there, 0.237 vs 0.225 ms)
+      // tile (the pair tile's 8-byte form was slower there, 0.237 vs 0.225 ms,
+      // and so was the TMA double-row kernel, 0.31 ms)
       if (var == 5 && h->plan_flag == B200FFT_PLAN_ESTIMATE && !f64 && p.ch.col &&
           p.ch.L == 512 && colpair_vec_ok(a))
         var = kVariantPair;
@@ -863,6 +864,12 @@ cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
           h->used_tma = true;
           h->last_tma = true;
           return launch_tma_col_c2c_f32(p.ch.L, fwd, var == kVariantTma ? 512 : 1024, a,
+                                        h->stream);
+        }
+        if (!f64 && p.ch.col && tma_mid_ok(p.ch.L, a)) {
+          h->used_tma = true;
+          h->last_tma = true;
+          return launch_tma_mid_c2c_f32(p.ch.L, fwd, var == kVariantTma ? 512 : 1024, a,
                                         h->stream);
         }
         var = default_variant(h->csize(), p.ch.L, p.ch.col, p.stride);

@@ -57,6 +57,9 @@ cudaError_t tc5col_take_fault(unsigned *fault);
 // stride), the launch (nt = 512 or 1024 threads per CTA) and the fault word.
 bool tma_col_ok(int L, const PassArgs &a);
 cudaError_t launch_tma_col_c2c_f32(int L, bool fwd, int nt, const PassArgs &a, cudaStream_t st);
+// the same for odd point strides (double-row map; FP32 256/512 points)
+bool tma_mid_ok(int L, const PassArgs &a);
+cudaError_t launch_tma_mid_c2c_f32(int L, bool fwd, int nt, const PassArgs &a, cudaStream_t st);
 cudaError_t tma_take_fault(unsigned *fault);
 
 // Pair-column C2C kernels (fs_colpair.cu, tile variant kVariantPair): FP32
