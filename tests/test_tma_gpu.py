@@ -138,7 +138,7 @@ def test_tma_odd_stride_columns(variant, length, widths, direction, monkeypatch)
         assert O.rel_l2(y, ref) < tol(nv.F32), (variant, length, w)
 
 
-@pytest.mark.parametrize("shape", [(24, 512, 512), (6, 256, 256), (5, 512, 36)])
+@pytest.mark.parametrize("shape", [(24, 512, 512), (6, 256, 256), (5, 512, 36), (7, 512, 60)])
 def test_tma_odd_stride_through_parafaft_r2c(shape, monkeypatch):
     """ParaFaFT_R2C on B200Backend<float> with the double-row kernel on the
     middle axis (variant 8): many slabs per launch (the slab coordinate of the
