@@ -853,7 +853,7 @@ cudaError_t launch_kernel(H *h, const Plan &p, int dir, const PassArgs &a) {
       // by default: 16-byte loads, stores and exchanges (512^3 first-axis
       // pass 0.212 -> 0.195 ms); odd point strides keep the one-transform
       // tile (the pair tile's 8-byte form was slower there, 0.237 vs 0.225 ms,
-      // and so was the TMA double-row kernel, 0.31 ms)
+      // and so was the TMA double-row kernel, 0.235 ms)
       if (var == 5 && h->plan_flag == B200FFT_PLAN_ESTIMATE && !f64 && p.ch.col &&
           p.ch.L == 512 && colpair_vec_ok(a))
         var = kVariantPair;

@@ -4,8 +4,10 @@
 // a padded R2C grid) through a map of double rows (fft_tma_mid_kernel below).
 // Both are autotuner candidates (tile variants 8 and 9): on the 512^3 R2C
 // step the ring ties the register-direct tile on the aligned first axis
-// (0.214 vs 0.212 ms) and the double-row kernel loses on the middle axis
-// (0.31 vs 0.228 ms; its box rows straddle 128-byte lines like plain loads).
+// (0.214 vs 0.212 ms) and the double-row kernels lose on the middle axis
+// (0.235 ms one CTA per tile, variant 8; the ring slower; 0.228 ms for the
+// register-direct tile: the odd rows' boxes read two extra columns and their
+// rows straddle 128-byte lines like plain loads).
 //
 // A persistent CTA per SM walks its tiles (TB adjacent transforms, 64 KiB)
 // through a ring of three shared-memory buffers. Thread 0 fills each buffer
@@ -29,6 +31,7 @@
 #include <cudaTypedefs.h>
 
 #include <atomic>
+#include <climits>
 #include <cstdint>
 #include <cstdlib>
 #include <mutex>
@@ -352,6 +355,114 @@ __global__ void __launch_bounds__(NT, 1)
   }
 }
 
+// The same tiles without the ring: one CTA per tile (68 KiB of shared memory,
+// two CTAs per SM), the two boxes of its tile waited for on one mbarrier. On
+// the 512^3 middle axis this form runs 0.235 ms against 0.29-0.32 ms for the
+// ring (one 512-thread CTA per SM leaves the stage barriers uncovered) and
+// 0.228 ms for the register-direct tile. The stall test hook skips the copies
+// of tile 0 only.
+template <int L, int NT, bool FWD>
+__global__ void __launch_bounds__(NT, 2)
+    fft_tma_mid_tile_kernel(const __grid_constant__ CUtensorMap map_even,
+                            const __grid_constant__ CUtensorMap map_odd, const PassArgs a, int q,
+                            long long n_main, int rem, int stall) {
+  using G = MidGeom<L>;
+  constexpr int TB = G::TB;
+  using K = KS<float, L, NT, TB, true, FWD, KIND_C2C, true>;
+  using V = typename K::V;
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  __shared__ __align__(8) unsigned long long full;
+  __shared__ int abort_flag;
+  const long long tile = blockIdx.x;
+  const long long W = a.istride;
+  const int tid = threadIdx.x;
+  typename K::Ctx c;
+  c.g = tid / TB;
+  c.tb = tid % TB;
+  c.tw = reinterpret_cast<const V *>(a.tw);
+  c.ist = a.istride;
+  c.ost = a.ostride;
+  c.gin = nullptr;
+  constexpr int R = K::S.rad[0];
+  constexpr int B = L / R;
+  constexpr int KB = (B + K::P - 1) / K::P;
+  constexpr bool FULL = (B % K::P) == 0;
+  V v[K::EMAX];
+  if (tile < n_main) {
+    const long long sl = tile / q;
+    const long long c0 = (tile - sl * q) * TB;
+    if (tid == 0) {
+      const uint32_t mb = su32(&full);
+      const uint32_t dst = su32(smraw);
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      const bool skip = stall && tile == 0;
+      if (!skip) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
+                     "r"(G::STAGE)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+            "l"(reinterpret_cast<uint64_t>(&map_even)), "r"(static_cast<int>(2 * c0)), "r"(0),
+            "r"(static_cast<int>(sl)), "r"(mb)
+            : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst + G::EVEN_BYTES),
+            "l"(reinterpret_cast<uint64_t>(&map_odd)), "r"(static_cast<int>(2 * (W + c0 - 1))),
+            "r"(0), "r"(static_cast<int>(sl)), "r"(mb)
+            : "memory");
+      }
+      abort_flag = 0;
+      if (!tma_wait(mb, 0)) {
+        abort_flag = 1;
+        atomicOr(&g_tma_fault, 1u);
+        if (!skip) // copies in flight: wait for them (bounded) before shared memory goes away
+          tma_wait(mb, 0);
+      }
+    }
+    __syncthreads();
+    if (abort_flag)
+      return;
+    V *const even = reinterpret_cast<V *>(smraw);
+    const V *const odd = even + G::EVEN_BYTES / 8 + 1 + c.tb;
+    c.sm = even;
+    c.act = true;
+    c.gout = reinterpret_cast<V *>(a.out) + sl * a.oslab + (c0 + c.tb) * a.odist;
+#pragma unroll
+    for (int i = 0; i < KB; ++i) {
+      const int j = c.g + K::P * i;
+      if (FULL || j < B) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int n = j + r * B;
+          v[i * R + r] = (n & 1) ? odd[(n >> 1) * G::ODD_W] : even[(n >> 1) * TB + c.tb];
+        }
+      }
+    }
+    K::template run<0>(c, v);
+  } else {
+    const long long b = (tile - n_main) * TB + c.tb;
+    const long long slabs = a.total / a.batch;
+    c.act = b < slabs * rem;
+    const long long sl = c.act ? b / rem : 0;
+    const long long col = static_cast<long long>(q) * TB + (c.act ? b - sl * rem : 0);
+    c.gin = reinterpret_cast<const V *>(a.in) + sl * a.islab + col * a.idist;
+    c.gout = reinterpret_cast<V *>(a.out) + sl * a.oslab + col * a.odist;
+    c.sm = reinterpret_cast<V *>(smraw);
+#pragma unroll
+    for (int i = 0; i < KB; ++i) {
+      const int j = c.g + K::P * i;
+      const bool ok = c.act && (FULL || j < B);
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        v[i * R + r] = ok ? c.gin[static_cast<long long>(j + r * B) * c.ist] : czero<V>();
+    }
+    K::template run<0>(c, v);
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
@@ -412,17 +523,25 @@ cudaError_t launch_tma_t(const PassArgs &a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// nt = 512: one CTA per tile (fft_tma_mid_tile_kernel); nt = 1024: persistent
+// CTAs through the ring (fft_tma_mid_kernel).
 template <int L, int NT, bool FWD>
 cudaError_t launch_tma_mid_t(const PassArgs &a, cudaStream_t st) {
   using G = MidGeom<L>;
   constexpr int TB = G::TB;
-  auto kern = fft_tma_mid_kernel<L, NT, FWD>;
+  constexpr bool kTile = NT == 512;
+  auto kern = [] {
+    if constexpr (kTile)
+      return fft_tma_mid_tile_kernel<L, NT, FWD>;
+    else
+      return fft_tma_mid_kernel<L, NT, FWD>;
+  }();
   static std::atomic<int> configured_mask{0}; // devices opted in
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 31 && !(configured_mask.load() & (1 << dev))) {
-    cudaError_t e =
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kTile ? G::STAGE : G::SMEM);
     if (e != cudaSuccess)
       return e;
     configured_mask.fetch_or(1 << dev);
@@ -459,12 +578,21 @@ cudaError_t launch_tma_mid_t(const PassArgs &a, cudaStream_t st) {
   const long long ntiles = n_main + n_rem;
   if (ntiles <= 0)
     return cudaSuccess;
-  const long long sms = sm_count();
-  const long long grid = ntiles < sms ? ntiles : sms;
   const char *sv = std::getenv("B200FFT_TMA_STALL_TEST");
   const int stall = (sv != nullptr && sv[0] == '1') ? 1 : 0;
-  kern<<<static_cast<unsigned>(grid), NT, G::SMEM, st>>>(map_even, map_odd, a, q, n_main, n_rem,
-                                                         rem, stall);
+  if constexpr (NT == 512) {
+    // one CTA per tile
+    if (ntiles > INT_MAX)
+      return cudaErrorInvalidConfiguration;
+    kern<<<static_cast<unsigned>(ntiles), NT, G::STAGE, st>>>(map_even, map_odd, a, q, n_main,
+                                                              rem, stall);
+  } else {
+    // persistent CTAs through the ring
+    const long long sms = sm_count();
+    const long long grid = ntiles < sms ? ntiles : sms;
+    kern<<<static_cast<unsigned>(grid), NT, G::SMEM, st>>>(map_even, map_odd, a, q, n_main, n_rem,
+                                                           rem, stall);
+  }
   return cudaGetLastError();
 }
 

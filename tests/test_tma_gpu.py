@@ -164,11 +164,13 @@ def test_tma_odd_stride_through_parafaft_r2c(shape, monkeypatch):
     f.close()
 
 
-def test_tma_odd_stride_wait_timeout_reports_device_status(monkeypatch):
-    """The stall hook on the double-row kernel: the first tile's copies are
-    skipped, its wait runs out, sync reports B200FFT_ERR_DEVICE_STATUS, and the
-    next launch on the same context is correct."""
-    monkeypatch.setenv("B200FFT_VARIANT", "8")
+@pytest.mark.parametrize("variant", [8, 9])
+def test_tma_odd_stride_wait_timeout_reports_device_status(variant, monkeypatch):
+    """The stall hook on the double-row kernels (variant 8: one CTA per tile,
+    tile 0's copies skipped; variant 9: the ring, every CTA's first tile): the
+    wait runs out, sync reports B200FFT_ERR_DEVICE_STATUS, and the next launch
+    on the same context is correct."""
+    monkeypatch.setenv("B200FFT_VARIANT", str(variant))
     length, w = 512, 257
     x = O.normal_complex((length - 1) * w + w, 12)
     h = nv.Handle(nv.F32, 1)
