@@ -124,6 +124,44 @@ def _run_record(script: str) -> str:
     return r.stdout
 
 
+
+def test_geometry_beyond_32_bit_counts_without_allocating():
+    """Plans and launches whose element counts pass 2^31 and 2^32 (as the
+    reference's geometry unit tests check its counts without allocating,
+    test/unit/test_exchange_geometry.cpp): a record-only handle never touches
+    the pointers, so the addresses below are never mapped. Rows of 4096
+    points over 2^20 + 3 transforms (2^32 + 12288 elements); 2^11 middle-axis
+    calls of 1024 x 1024 slabs coalesced into one launch (2^31 elements); an
+    R2C pass of 2^19 + 1 rows of 8192 reals."""
+    h = nv.Handle(nv.F32, 2, flags=nv.FLAG_RECORD_ONLY)
+    base = 1 << 40
+    rows = (1 << 20) + 3
+    h.plan_c2c(0, 4096, rows, 1, 4096)
+    h.exec_c2c(0, nv.FORWARD, base)
+    r = h.log()[-1]
+    assert r["transforms"] == rows and r["slabs"] == 1
+    assert r["bytes"] == 2 * 4096 * rows * 8 > 2 ** 32
+    # middle axis: the last-axis plan makes the stage buffer 2^31 elements, so
+    # consecutive slab calls coalesce (infer_lead) into one pass of 2048 slabs
+    h.plan_c2c(0, 1024, 1 << 21, 1, 1024)
+    h.plan_c2c(1, 1024, 1024, 1024, 1)
+    slab_bytes = 1024 * 1024 * 8
+    for k in range(2048):
+        h.exec_c2c(1, nv.BACKWARD, base + k * slab_bytes)
+    r = h.log()[-1]
+    assert (r["stage"], r["slabs"], r["transforms"]) == (1, 2048, 1024 * 2048)
+    assert r["bytes"] == 2 * (1 << 31) * 8
+    st = h.stats()
+    assert st["coalesced_calls"] == 2047 and st["kernel_launches"] == 2
+    # R2C rows: 8192 reals each, padded to 8194
+    rr = (1 << 19) + 1
+    h.plan_r2c(8192, rr, 1, 8194)
+    h.exec_r2c(base)
+    r = h.log()[-1]
+    assert r["kind"] == nv.KIND_R2C and r["transforms"] == rr
+    assert r["bytes"] == rr * (8192 * 4 + 4097 * 8) > 2 ** 32
+    h.close()
+
 def _drivers_built():
     return nv.DRIVERS_PATH.exists()
 
