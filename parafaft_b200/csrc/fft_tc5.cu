@@ -31,7 +31,6 @@
 #include <cuda_fp16.h>
 
 #include <stdint.h>
-#include <cstdio>
 #include <atomic>
 #include <cstdlib>
 
@@ -274,17 +273,10 @@ cudaError_t launch_tc5_row256_f32(bool fwd, const PassArgs &a, cudaStream_t st) 
     cudaError_t e = cudaFuncGetAttributes(&fa, kern);
     if (e != cudaSuccess)
       return e;
-    int nb = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kTc5Threads, 0);
-    if (e != cudaSuccess)
-      return e;
     const int by_regs = fa.numRegs > 0 ? 65536 / (fa.numRegs * kTc5Threads) : 8;
     const int by_smem = static_cast<int>((227 * 1024) / (fa.sharedSizeBytes + 1024));
     int n = by_regs < by_smem ? by_regs : by_smem;
     n = n > 512 / static_cast<int>(kTc5Cols) ? 512 / static_cast<int>(kTc5Cols) : n;
-    if (std::getenv("B200FFT_DEBUG_OCC"))
-      std::fprintf(stderr, "tc5 occupancy: api %d regs %d smem %zu -> %d\n", nb, fa.numRegs,
-                   fa.sharedSizeBytes, n);
     per_sm[dev] = n < 1 ? 1 : n;
   }
   int sms = 0;
