@@ -948,7 +948,14 @@ def run_b200(args):
             torch.cuda.empty_cache()
 
     if rank == 0:
-        cpu_ms, cpu_n, cores = time_cpu(host_buf, budget_s=args.cpu_budget, max_steps=8)
+        # the CPU baseline is timed at N = 1 only (at N > 1 the other ranks
+        # would wait on it at the closing barrier)
+        cpu = None
+        if world == 1:
+            cpu_ms, cpu_n, cores = time_cpu(host_buf, budget_s=args.cpu_budget, max_steps=8)
+            cpu = {"value": round(cpu_ms, 1), "unit": "ms", "cores": cores, "kind": "port",
+                   "sample": f"{cpu_n} full 512^3 fwd+bwd steps, scipy.fft float32 "
+                             f"(FFTWBackend<float> stand-in: libfftw3f absent)"}
         nbytes = host_buf.nbytes
         line = {
             "metric": METRIC, "value": round(ms, 4), "unit": "ms", "n_gpus": world,
@@ -978,9 +985,7 @@ def run_b200(args):
             "configs": configs if configs is not None else "headline only (N > 1 replicas or --headline-only)",
             "gpu_launches": int(launches),
             "clocks": clk,
-            "cpu_baseline": {"value": round(cpu_ms, 1), "unit": "ms", "cores": cores, "kind": "port",
-                             "sample": f"{cpu_n} full 512^3 fwd+bwd steps, scipy.fft float32 "
-                                       f"(FFTWBackend<float> stand-in: libfftw3f absent)"},
+            "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     if configs is None:
