@@ -2057,6 +2057,11 @@ int group_build(G *g) {
       s.smem = std::max(s.smem, generic_smem_bytes(f64, ga.TB, ga.L));
       s.bytes += pass_bytes(h, p, ga.p.total);
     }
+    // largest launches first: the level's launches take the chain's lanes
+    // round robin, so each lane starts with a long one and the short ones
+    // fill in behind
+    std::stable_sort(g->steps.begin() + static_cast<std::ptrdiff_t>(first_step), g->steps.end(),
+                     [](const GroupStep &a, const GroupStep &b) { return a.bytes > b.bytes; });
     for (size_t i = first_step; i < g->steps.size(); ++i) {
       g->steps[i].level = static_cast<int>(d);
       g->steps[i].chain = chain;
