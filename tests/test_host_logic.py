@@ -116,6 +116,45 @@ def test_fastdiv_restatement():
             assert q == n // d, (n, d)
 
 
+
+def test_double_row_box_geometry_restatement():
+    """The tile geometry of the TMA double-row column kernels (fft_tma.cu,
+    MidGeom and the box coordinates), restated and checked on every odd point
+    stride W that tma_mid_ok admits up to 1025 (and 512^3's 257): a map of
+    double rows {4W floats, L/2 rows}; tile c0 = k*TB takes its even point rows
+    from a box of TB columns at x = c0 and its odd ones from a box of TB + 2
+    columns at x = W + c0 - 1. Both boxes start on a 16-byte boundary (x * 8
+    bytes), stay inside the double row, and together hold exactly the tile's
+    TB columns of every point row at the offsets the kernel reads (column
+    1 + t of the odd box); the W mod TB columns left over go to remainder
+    tiles, so every column of every row is read by exactly one tile."""
+    tile_bytes = 64 * 1024
+    for L in (256, 512):
+        TB = tile_bytes // (L * 8)
+        half = L // 2
+        even_b = TB * half * 8
+        odd_w = TB + 2
+        stage = even_b + odd_w * half * 8
+        assert half <= 256 and stage >= tile_bytes and even_b % 128 == 0 and stage % 128 == 0
+        assert 3 * stage <= 227 * 1024
+        for W in [w for w in range(TB + 2, 1026) if w % 2 == 1] + [257]:
+            q, rem = divmod(W, TB)
+            seen = [0] * W
+            for k in range(q):
+                c0 = k * TB
+                x_even, x_odd = c0, W + c0 - 1          # complex columns in the double row
+                assert (x_even * 8) % 16 == 0 and (x_odd * 8) % 16 == 0
+                assert x_even + TB <= 2 * W and x_odd + odd_w <= 2 * W
+                for t in range(TB):
+                    # even point row 2m: double-row column x_even + t = point column c0 + t
+                    assert x_even + t == c0 + t
+                    # odd point row 2m+1: double-row column W + (c0 + t) = x_odd + 1 + t
+                    assert W + c0 + t == x_odd + 1 + t
+                    seen[c0 + t] += 1
+            for b in range(rem):                          # one slab's remainder columns
+                seen[q * TB + b] += 1
+            assert seen == [1] * W, (L, W)
+
 def _run_record(script: str) -> str:
     env = dict(os.environ, B200FFT_RECORD_ONLY="1")
     r = subprocess.run([sys.executable, "-c", script], env=env, capture_output=True,
