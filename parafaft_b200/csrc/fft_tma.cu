@@ -1,7 +1,8 @@
 // TMA-fed column passes: FP32 C2C of 256, 512 or 1024 points whose point
 // rows are 16-byte aligned (ParaFaFT's first axis, and middle axes of even
 // width), and of 256 or 512 points at an odd point stride (the middle axis of
-// a padded R2C grid) through a map of double rows (fft_tma_mid_kernel below).
+// a padded R2C grid) through a map of double rows (fft_tma_mid_tile_kernel,
+// one CTA per tile, and fft_tma_mid_kernel, the ring form, below).
 // Both are autotuner candidates (tile variants 8 and 9): on the 512^3 R2C
 // step the ring ties the register-direct tile on the aligned first axis
 // (0.214 vs 0.212 ms) and the double-row kernels lose on the middle axis
@@ -24,9 +25,10 @@
 // Every wait on a buffer's barrier is bounded by the clock (about a second);
 // past it the CTA sets g_tma_fault, waits (bounded) for the copies it still
 // has in flight and returns, and b200fft_sync reports
-// B200FFT_ERR_DEVICE_STATUS. B200FFT_TMA_STALL_TEST=1 makes every CTA skip the
-// copies of its first tile, so that first wait runs out (the test of this
-// path: nothing faults, the context stays usable).
+// B200FFT_ERR_DEVICE_STATUS. B200FFT_TMA_STALL_TEST=1 makes every ring CTA
+// skip the copies of its first tile (the one-CTA-per-tile form: tile 0's), so
+// that wait runs out (the test of this path: nothing faults, the context stays
+// usable).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -197,7 +199,7 @@ __global__ void __launch_bounds__(NT, 1)
 // (TB columns, 16-byte aligned since c0 is even) and the odd rows at
 // x = W + c0 - 1 (even, so aligned), TB + 2 columns wide; the odd rows' points
 // sit one column into that box. Both boxes are L/2 rows high and land side by
-// side in one ring buffer. The W mod TB columns left over at the end of each
+// side in one 68 KiB buffer. The W mod TB columns left over at the end of each
 // row (one column at W = 257) form remainder tiles after every slab's full
 // tiles: TB such columns of different slabs per tile, loaded with plain loads,
 // transformed and stored like the others.
